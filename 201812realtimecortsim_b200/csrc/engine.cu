@@ -1,0 +1,1668 @@
+// engine.cu -- the B200 engine: connectome build, bath producer, delivery,
+// LIFCA update, spike compaction and STDP, behind the C ABI of
+// include/dpsnn_b200.h.
+//
+// Arithmetic follows the reference operation by operation (compiled with
+// --fmad=false so no multiply-add is contracted, like the reference's
+// x86-64 SSE2 build); the comments cite the reference lines each kernel
+// restates.  Data layout in HBM (N neurons, S synapses, D delays):
+//   neuron state  SoA fp64 v, c, Tr, Te, nextBath (5*8 B/neuron)
+//   connectome    CSR sorted by (pre, delay, generation order):
+//                 row_ptr[N+1] u64, sub_off[N*(D+1)] u16 (per-delay offsets
+//                 inside a row), post[S] u32, w16[S] i16 (6 B/synapse);
+//                 with STDP also tderiv[S] f32, last_act[S] i32
+//   spike ring    80 slots x N: ids u32, te f64 (one slot per step)
+//   events        per target neuron `cap` slots of {u32 key, f32 weight};
+//                 overflow list of {target, key, weight}
+//   bath          per rank: 64-entry ran3 history, draw ring of LUT index
+//                 (u8) and lapse (f32); per step per-neuron event lists
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <dlfcn.h>
+#include <string>
+#include <vector>
+
+#include "dd_math.cuh"
+#include "dpsnn_internal.h"
+
+#define RING_SLOTS 80          // DSD__maxD: axonal delay ring length
+#define MAX_SYN_PER_NEURON 7500  // DSD__maxM (Makefile miniM)
+#define MAX_INPUTS_PER_STEP 6000 // DSD__maxSimultaneousSpikesOnSameTarget
+#define MBIG 1000000000
+#define MSEED 161803398
+#define DRAW_RING (1u << 16)   // bath draws buffered per rank
+#define NEURON_BLOCK 256
+#define LOCAL_EVENTS 64        // per-thread event buffer of the neuron kernel
+
+// ------------------------------------------------------------------ errors
+static thread_local char g_err[1024];
+int dpsnn_fail(int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof g_err, fmt, ap);
+  va_end(ap);
+  return code;
+}
+extern "C" const char *dpsnn_last_error(void) { return g_err; }
+
+const char *dpsnn_library_dir(void) {
+  static std::string dir;
+  if (dir.empty()) {
+    Dl_info info;
+    if (dladdr((void *)&dpsnn_library_dir, &info) && info.dli_fname) {
+      dir = info.dli_fname;
+      size_t p = dir.rfind('/');
+      dir = (p == std::string::npos) ? std::string(".") : dir.substr(0, p);
+    } else {
+      dir = ".";
+    }
+  }
+  return dir.c_str();
+}
+
+#define CK(x)                                                                       \
+  do {                                                                              \
+    cudaError_t e_ = (x);                                                           \
+    if (e_ != cudaSuccess)                                                          \
+      return dpsnn_fail(DPSNN_E_CUDA, "%s: %s", #x, cudaGetErrorString(e_));        \
+  } while (0)
+
+// Error flags raised by kernels (bit set in Dev::flags[0]).
+enum {
+  F_TIME_WINDOW = 1,     // event time outside [t, t+1)  (DPSNN_neuron_sim.c:681-685)
+  F_NO_TARGET = 2,       // spiking neuron without targets (DPSNN_localNet_sim.c:732-737)
+  F_OVERFLOW = 4,        // overflow list full
+  F_TOO_MANY_INPUTS = 8, // > miniSimSpikes inputs on one neuron in one step
+  F_BATH_DRAWS = 16,     // bath draw ring exhausted
+  F_GEN = 32,            // synapse generation error (see gen error code)
+};
+
+// ------------------------------------------------------------------ model
+struct NetConst {
+  uint32_t N, locN, P, D, nsub, npcm, cfx, cfy, nmod, mods_per_rank;
+  uint32_t stencil, max_mod, stencil_dim, delay_min, delay_max;
+  uint32_t offset[DPSNN_MAX_SUBPOP], count[DPSNN_MAX_SUBPOP];
+  double Tau[DPSNN_MAX_SUBPOP], Theta[DPSNN_MAX_SUBPOP], H[DPSNN_MAX_SUBPOP];
+  double Tarp[DPSNN_MAX_SUBPOP], AlphaC[DPSNN_MAX_SUBPOP], TauC[DPSNN_MAX_SUBPOP];
+  double gC[DPSNN_MAX_SUBPOP], NuExt[DPSNN_MAX_SUBPOP];
+  double J[DPSNN_MAX_SUBPOP * DPSNN_MAX_SUBPOP], DJ[DPSNN_MAX_SUBPOP * DPSNN_MAX_SUBPOP];
+  double DMin[DPSNN_MAX_SUBPOP * DPSNN_MAX_SUBPOP], DMax[DPSNN_MAX_SUBPOP * DPSNN_MAX_SUBPOP];
+  float f2w, w2f, min_w;
+  uint32_t global_seed, start_pl, stop_pl, stdp_on;
+  float causal_tab[128], anti_tab[128];
+  float stdp_drift, stdp_tauDecay;
+  uint32_t ev_cap, ovf_cap;
+  uint32_t bath_need;  // draws kept ahead of the bath consumer
+};
+
+// ------------------------------------------------------------------ ran3
+// Numerical Recipes ran3 with the reference's |mj| tweak and seeding rules
+// (randdev.c:116-196, :477-502).  Same code on host and device.
+struct Ran3 {
+  int32_t ma[56];
+  int32_t inext, inextp, iff, idum;
+};
+
+__host__ __device__ static inline double r3_rand(Ran3 &g) {
+  int32_t mj, mk;
+  if (g.idum < 0 || g.iff == 0) {
+    g.iff = 1;
+    mj = MSEED - (g.idum < 0 ? -g.idum : g.idum);
+    mj = (mj < 0 ? -mj : mj);
+    mj %= MBIG;
+    g.ma[55] = mj;
+    mk = 1;
+    for (int i = 1; i <= 54; i++) {
+      int ii = (21 * i) % 55;
+      g.ma[ii] = mk;
+      mk = mj - mk;
+      if (mk < 0) mk += MBIG;
+      mj = g.ma[ii];
+    }
+    for (int k = 1; k <= 4; k++)
+      for (int i = 1; i <= 55; i++) {
+        g.ma[i] -= g.ma[1 + (i + 30) % 55];
+        if (g.ma[i] < 0) g.ma[i] += MBIG;
+      }
+    g.inext = 0;
+    g.inextp = 31;
+    g.idum = 1;
+  }
+  if (++g.inext == 56) g.inext = 1;
+  if (++g.inextp == 56) g.inextp = 1;
+  mj = g.ma[g.inext] - g.ma[g.inextp];
+  if (mj < 0) mj += MBIG;
+  g.ma[g.inext] = mj;
+  return mj * (1.0 / (double)MBIG);
+}
+__host__ __device__ static inline void r3_seed(Ran3 &g, int32_t s) {
+  g.idum = -s;
+  (void)r3_rand(g);
+}
+// The last 55 outputs (oldest first): the whole state of the lagged
+// Fibonacci recurrence x[n] = x[n-55] - x[n-24] (mod 1e9) that ran3 runs.
+__host__ __device__ static inline void r3_history(const Ran3 &g, uint32_t *hist55) {
+  int k = 0;
+  for (int i = g.inext + 1; i <= 55; i++) hist55[k++] = (uint32_t)g.ma[i];
+  for (int i = 1; i <= g.inext; i++) hist55[k++] = (uint32_t)g.ma[i];
+}
+
+struct NormState {
+  int32_t set;
+  double cache;
+};
+// NormDev: polar Box-Muller with a one-value cache (randdev.c:584-606).
+__device__ static inline double normdev(Ran3 &g, NormState &ns) {
+  if (ns.set == 0) {
+    double v1, v2, r, fac;
+    do {
+      v1 = (double)(2.0 * r3_rand(g) - 1.0);
+      v2 = (double)(2.0 * r3_rand(g) - 1.0);
+      r = v1 * v1 + v2 * v2;
+    } while (r >= 1.0 || r == 0.0);
+    fac = (double)sqrt(-2.0 * log_cr(r) / r);
+    ns.cache = v1 * fac;
+    ns.set = 1;
+    return v2 * fac;
+  }
+  ns.set = 0;
+  return ns.cache;
+}
+
+__host__ __device__ static inline uint32_t roundr2i(double r) {  // erflib.c:172-181
+  double i = floor(r);
+  if (i + 0.5 > r) return (uint32_t)i;
+  return (uint32_t)(i + 1.0);
+}
+
+__device__ static inline uint32_t subpop_of(const NetConst *net, uint32_t in_cm) {
+  for (uint32_t s = 0; s < net->nsub; s++)
+    if (in_cm >= net->offset[s] && in_cm < net->offset[s] + net->count[s]) return s;
+  return 0xFFFFFFFFu;
+}
+
+// ------------------------------------------------------------------ generation
+// One thread walks one cortical module's neurons in order, consuming that
+// module's serial ran3 stream exactly as simpleCM_invokeIndivSynGenerators
+// (DPSNN_LIFCAcorticalModuleGen.cpp:62-220) does.  Modules are independent
+// streams (SetRandomSeed(module) at :96-107) except for NormDev's cached
+// value, which carries from one module to the next inside a rank; pass A runs
+// each module under both hypotheses for that cache (empty, or holding a value
+// that the module's first weight accepts) and pass B regenerates the chosen
+// one, writing synapses straight into their CSR slots.
+struct GenRecord {
+  uint32_t nsyn;
+  int32_t used_normdev, set_out, err;
+  double cache_out;
+  float first_mean, first_sigma;
+  uint32_t err_arg;
+  uint32_t hist[55];
+};
+
+enum { GEN_ERR_TOO_MANY = 1, GEN_ERR_WEIGHT_RANGE = 2, GEN_ERR_PROB = 3, GEN_ERR_DELAY = 4,
+       GEN_ERR_ZERO_MEAN = 5 };
+
+__device__ static inline uint32_t empty_random_synapses(Ran3 &g, float pf, uint32_t max_n) {
+  // getEmptyRandomSynapses (DPSNN_LIFCAconnectome.cpp:1079-1133)
+  double connectivity = (double)pf;
+  double r = r3_rand(g);
+  double P = connectivity, C = P;
+  uint32_t n = 1;
+  while ((C < r) && (n <= max_n)) {
+    n++;
+    P *= 1 - connectivity;
+    C += P;
+  }
+  return n;
+}
+
+__device__ static inline uint32_t random_delay_uni(const NetConst *net, Ran3 &g, uint32_t s, uint32_t t) {
+  // getRandomDelay_UNI (DPSNN_LIFCAcorticalModuleGen.cpp:299-338)
+  float outF, DMin, DMax, DelayMin, DelayMax, DelayStep, DelayNum;
+  DMin = (float)net->DMin[s * DPSNN_MAX_SUBPOP + t];
+  DMax = (float)net->DMax[s * DPSNN_MAX_SUBPOP + t];
+  DelayMin = (float)net->delay_min;
+  DelayMax = (float)net->delay_max;
+  DelayNum = 80;
+  DelayStep = (DelayMax - DelayMin) / DelayNum;
+  DelayMax -= DelayStep / 2;
+  DelayMin += DelayStep / 2;
+  DMax = roundr2i((DMax - DelayMin) / DelayStep) * DelayStep + DelayMin;
+  DMin = roundr2i((DMin - DelayMin) / DelayStep) * DelayStep + DelayMin;
+  outF = (float)((r3_rand(g) * (DMax - DMin) + DMin - DelayMin) / DelayStep);
+  (void)DelayMax;
+  return roundr2i(outF * DelayStep);
+}
+
+__global__ void gen_kernel(const NetConst *__restrict__ net, const float *__restrict__ prob, int pass,
+                           GenRecord *rec, const int32_t *__restrict__ chosen_hyp,
+                           const double *__restrict__ chosen_cache, uint16_t *cnt_out,
+                           const uint64_t *__restrict__ row_ptr, const uint16_t *__restrict__ sub_off,
+                           uint32_t *post, int16_t *w16, uint32_t *scratch,
+                           const uint32_t *__restrict__ bath_tmpl, double *inv_nu,
+                           uint32_t *max_ext, uint8_t *sub) {
+  uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t nthreads = (pass == 0) ? 2 * net->nmod : net->nmod;
+  if (tid >= nthreads) return;
+  uint32_t m = (pass == 0) ? (tid >> 1) : tid;
+  int hyp = (pass == 0) ? (int)(tid & 1) : chosen_hyp[m];
+  GenRecord *R = &rec[(pass == 0) ? tid : m];
+  const uint32_t N = net->N, D = net->D, npcm = net->npcm, stencil = net->stencil;
+  uint32_t *tl = scratch + (size_t)tid * MAX_SYN_PER_NEURON;
+  uint16_t cnt[RING_SLOTS];
+
+  Ran3 g;
+  g.iff = 0;
+  g.idum = 0;
+  g.inext = g.inextp = 0;
+  if (m % net->mods_per_rank == 0) r3_seed(g, (int32_t)net->global_seed);  // localNet_init.c:119
+  r3_seed(g, (int32_t)m);  // module start (ModuleGen.cpp:96-107); m==0 does not re-initialise
+  NormState ns;
+  ns.set = hyp;
+  ns.cache = (pass == 1 && hyp == 1) ? chosen_cache[m] : 0.0;
+  int used = 0;
+  uint32_t nsyn = 0;
+  R->err = 0;
+  for (uint32_t gi = m * npcm; gi < (m + 1) * npcm; gi++) {
+    uint32_t mod = gi / npcm;
+    uint32_t cfy = mod / net->cfx, cfx = mod % net->cfx;
+    uint32_t ssub = subpop_of(net, gi % npcm);
+    if (pass == 1) sub[gi] = (uint8_t)ssub;
+    uint32_t tot = 0;
+    for (uint32_t ts = 0; ts < net->nsub; ts++)
+      for (uint32_t x = 0; x < stencil; x++)
+        for (uint32_t y = 0; y < stencil; y++) {
+          int32_t nx = (int32_t)cfx + (int32_t)x - (int32_t)net->max_mod;
+          int32_t ny = (int32_t)cfy + (int32_t)y - (int32_t)net->max_mod;
+          if (nx < 0 || nx >= (int32_t)net->cfx || ny < 0 || ny >= (int32_t)net->cfy) continue;
+          float pf = prob[(((size_t)ssub * DPSNN_MAX_SUBPOP + ts) * stencil + x) * stencil + y];
+          if (!(pf > 0)) continue;
+          if (!(pf > 0.00001f)) { R->err = GEN_ERR_PROB; R->err_arg = gi; return; }
+          uint32_t in_cm = net->offset[ts] - 1;
+          uint32_t last = net->offset[ts] + net->count[ts];
+          uint32_t avail = last - in_cm;
+          while ((in_cm += empty_random_synapses(g, pf, avail)) < last) {
+            if (tot >= MAX_SYN_PER_NEURON) { R->err = GEN_ERR_TOO_MANY; R->err_arg = gi; return; }
+            tl[tot++] = in_cm + (uint32_t)nx * npcm + (uint32_t)ny * npcm * net->cfx;
+          }
+        }
+    if (tot >= MAX_SYN_PER_NEURON) { R->err = GEN_ERR_TOO_MANY; R->err_arg = gi; return; }
+    for (uint32_t d = 0; d < D; d++) cnt[d] = 0;
+    for (uint32_t j = 0; j < tot; j++) {
+      uint32_t tg = tl[j];
+      uint32_t tsub = subpop_of(net, tg % npcm);
+      uint32_t delay = random_delay_uni(net, g, ssub, tsub);
+      if (delay >= D) { R->err = GEN_ERR_DELAY; R->err_arg = delay; return; }
+      float mean = (float)net->J[ssub * DPSNN_MAX_SUBPOP + tsub];
+      float sigma = (float)(net->DJ[ssub * DPSNN_MAX_SUBPOP + tsub] * (double)mean);
+      if (!used) {
+        used = 1;
+        R->first_mean = mean;
+        R->first_sigma = sigma;
+      }
+      float wf;
+      if (mean > 0.0) {
+        do { wf = (float)(mean + normdev(g, ns) * sigma); } while ((wf < 0.0) || (wf >= 2.0 * mean));
+      } else {
+        if (mean == 0.0f) { R->err = GEN_ERR_ZERO_MEAN; R->err_arg = gi; return; }
+        do { wf = (float)(mean + normdev(g, ns) * sigma); } while ((wf <= 2.0 * mean) || (wf > 0));
+      }
+      if ((wf < net->min_w) || (wf > (-net->min_w))) { R->err = GEN_ERR_WEIGHT_RANGE; R->err_arg = gi; return; }
+      int16_t w = (int16_t)(wf * net->f2w);
+      if (pass == 0) {
+        cnt[delay]++;
+      } else {
+        uint64_t pos = row_ptr[gi] + sub_off[(size_t)gi * (D + 1) + delay] + cnt[delay]++;
+        post[pos] = tg;
+        w16[pos] = w;
+      }
+      nsyn++;
+    }
+    if (pass == 0) {
+      uint16_t *co = cnt_out + ((size_t)hyp * N + gi) * D;
+      for (uint32_t d = 0; d < D; d++) co[d] = cnt[d];
+    } else {
+      // external bath rate (ModuleGen.cpp:201-211, LIFCAconnectome.cpp:871-887)
+      float nu = (float)net->NuExt[ssub];
+      uint32_t bx = cfx, by = cfy;
+      if (bx >= net->cfx / 2) bx = -1 * (bx - net->cfx + 1);
+      if (by >= net->cfy / 2) by = -1 * (by - net->cfy + 1);
+      if (bx >= net->stencil_dim) bx = net->stencil_dim - 1;
+      if (by >= net->stencil_dim) by = net->stencil_dim - 1;
+      float cext = (float)bath_tmpl[bx * net->stencil_dim + by];
+      if (cext != 0) {
+        double inv = 1000.0 / (nu * cext);
+        inv_nu[gi] = inv;
+        max_ext[gi] = (uint32_t)ceil(20 / inv);
+      } else {
+        inv_nu[gi] = 0;
+        max_ext[gi] = 0;
+      }
+    }
+  }
+  R->nsyn = nsyn;
+  R->used_normdev = used;
+  R->set_out = ns.set;
+  R->cache_out = ns.cache;
+  r3_history(g, R->hist);
+}
+
+// ------------------------------------------------------------------ step kernels
+struct Dev {
+  NetConst *net;
+  double *lut;              // [nsub*256]
+  // neurons
+  double *v, *c, *tr, *te, *nb, *inv_nu;
+  uint32_t *max_ext;
+  uint8_t *sub, *fired;
+  int32_t *last_spike_ms;
+  uint32_t *block_fired;    // per NEURON_BLOCK block
+  // connectome
+  uint64_t *row_ptr;
+  uint16_t *sub_off;
+  uint32_t *post;
+  int16_t *w16;
+  float *tderiv;
+  int32_t *last_act;
+  uint64_t *in_ptr;
+  uint32_t *in_idx;
+  // ring
+  uint32_t *ring_ids, *ring_cnt;
+  double *ring_te;
+  // events
+  uint32_t *ev_cnt;
+  uint2 *ev;
+  uint32_t *ovf_cnt;
+  uint4 *ovf;
+  uint32_t *heavy_list, *heavy_cnt;
+  uint2 *heavy_scratch;     // {key, w} gathered for heavy neurons
+  double *heavy_tau;
+  uint32_t *heavy_scratch_used;
+  uint64_t heavy_scratch_cap;
+  // bath
+  uint32_t *bath_hist;      // [P][64] ran3 history ring
+  uint64_t *bath_produced, *bath_pos;  // [P]
+  uint8_t *draw_idx;        // [P][DRAW_RING]
+  float *draw_lapse;        // [P][DRAW_RING]
+  uint64_t *bath_rank_base; // [P+1]
+  uint32_t *bath_off;       // [N]
+  uint16_t *bath_cnt;       // [N]
+  double *bath_time;
+  uint8_t *bath_lut;
+  logf_fixup_t fix;
+  // control
+  uint32_t *t;              // current step
+  uint32_t *flags;
+  unsigned long long *events;  // synaptic events delivered
+};
+
+// Step 1: ordered spike compaction (compressNeuralSpikesInThisTimeStep,
+// DPSNN_localNet_sim.c:103-132, :620-664): the neurons that fired during the
+// previous step, ascending index, with their emission time Te, into ring slot
+// t mod 80.  Also sets lastNeuralEmittedSpikeTime_ms = t.
+__global__ void compact_kernel(Dev d) {
+  const NetConst *net = d.net;
+  const uint32_t N = net->N, t = *d.t, slot = t % RING_SLOTS;
+  const uint32_t b = blockIdx.x, nb = gridDim.x;
+  __shared__ uint32_t s_red[NEURON_BLOCK / 32];
+  __shared__ uint32_t s_prefix;
+  uint32_t part = 0;
+  for (uint32_t k = threadIdx.x; k < b; k += blockDim.x) part += d.block_fired[k];
+  for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = part;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t s = 0;
+    for (int w = 0; w < NEURON_BLOCK / 32; w++) s += s_red[w];
+    s_prefix = s;
+  }
+  __syncthreads();
+  uint32_t i = b * NEURON_BLOCK + threadIdx.x;
+  uint32_t f = (i < N) ? d.fired[i] : 0;
+  uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t bal = __ballot_sync(0xffffffffu, f);
+  __shared__ uint32_t s_wcnt[NEURON_BLOCK / 32];
+  if (lane == 0) s_wcnt[warp] = __popc(bal);
+  __syncthreads();
+  uint32_t woff = 0;
+  for (uint32_t w = 0; w < warp; w++) woff += s_wcnt[w];
+  if (f) {
+    uint32_t q = s_prefix + woff + __popc(bal & ((1u << lane) - 1));
+    d.fired[i] = 0;
+    d.ring_ids[(size_t)slot * N + q] = i;
+    d.ring_te[(size_t)slot * N + q] = d.te[i];
+    d.last_spike_ms[i] = (int32_t)t;
+    if (d.row_ptr[i + 1] == d.row_ptr[i]) atomicOr(d.flags, F_NO_TARGET);
+  }
+  if (b == nb - 1 && threadIdx.x == 0) {
+    uint32_t tot = s_prefix;
+    for (int w = 0; w < NEURON_BLOCK / 32; w++) tot += s_wcnt[w];
+    d.ring_cnt[slot] = tot;
+  }
+}
+
+// Causal STDP at detection (causalSTDP_ms_ofBackwardSynapses,
+// DPSNN_neuron_sim.c:94-177): one warp per spiking neuron walks its incoming
+// synapses.
+__global__ void causal_stdp_kernel(Dev d) {
+  const NetConst *net = d.net;
+  const uint32_t t = *d.t;
+  if (!(t >= net->start_pl && t <= net->stop_pl)) return;
+  const uint32_t slot = t % RING_SLOTS, cnt = d.ring_cnt[slot], N = net->N;
+  const uint32_t lane = threadIdx.x & 31;
+  for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < cnt;
+       w += (gridDim.x * blockDim.x) >> 5) {
+    uint32_t i = d.ring_ids[(size_t)slot * N + w];
+    for (uint64_t k = d.in_ptr[i] + lane; k < d.in_ptr[i + 1]; k += 32) {
+      uint32_t s = d.in_idx[k];
+      int32_t la = d.last_act[s];
+      int td = (int)t - 1 - la;
+      float fc = (la != 0 && td < 128) ? net->causal_tab[td] : 0.0f;
+      d.tderiv[s] = d.tderiv[s] + fc;
+    }
+  }
+}
+
+// Step 2: delivery (axonalSpikeSchedulersToSynapticSpikeSchedulers,
+// DPSNN_localNet_sim.c:837-999, and findAndGetNextSyn, DPSNN_synapse.c:179-267).
+// Work item = (delay d, spike q of the slot written d steps ago); one warp
+// walks the CSR segment (pre, d) and appends {key, weight} to each target's
+// event list.  key = (D-1-d) << 25 | q orders a target's events as the
+// reference delivers them (delay descending, then source ascending), which
+// breaks ties between equal arrival times.
+__global__ void deliver_kernel(Dev d) {
+  const NetConst *net = d.net;
+  const uint32_t t = *d.t, N = net->N, D = net->D, cap = net->ev_cap;
+  __shared__ uint32_t s_pre[RING_SLOTS + 1];
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0;
+    for (uint32_t dd = 0; dd < D; dd++) {
+      s_pre[dd] = acc;
+      acc += d.ring_cnt[(t + RING_SLOTS - dd) % RING_SLOTS];
+    }
+    s_pre[D] = acc;
+  }
+  __syncthreads();
+  const uint32_t total = s_pre[D];
+  const uint32_t lane = threadIdx.x & 31;
+  const bool stdp = net->stdp_on && t >= net->start_pl && t <= net->stop_pl;
+  const float w2f = net->w2f;
+  unsigned long long my_events = 0;
+  for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < total;
+       w += (gridDim.x * blockDim.x) >> 5) {
+    uint32_t dl = 0;
+    while (s_pre[dl + 1] <= w) dl++;
+    uint32_t q = w - s_pre[dl];
+    uint32_t slot = (t + RING_SLOTS - dl) % RING_SLOTS;
+    uint32_t P = d.ring_ids[(size_t)slot * N + q];
+    uint64_t base = d.row_ptr[P];
+    const uint16_t *so = d.sub_off + (size_t)P * (D + 1);
+    uint64_t beg = base + so[dl], end = base + so[dl + 1];
+    uint32_t key = ((D - 1 - dl) << 25) | q;
+    my_events += end - beg;
+    for (uint64_t k = beg + lane; k < end; k += 32) {
+      uint32_t j = d.post[k];
+      float wf = ((float)d.w16[k]) * w2f;
+      uint32_t s = atomicAdd(&d.ev_cnt[j], 1u);
+      if (s < cap) {
+        d.ev[(size_t)j * cap + s] = make_uint2(key, __float_as_uint(wf));
+      } else {
+        uint32_t o = atomicAdd(d.ovf_cnt, 1u);
+        if (o < net->ovf_cap)
+          d.ovf[o] = make_uint4(j, key, __float_as_uint(wf), 0u);
+        else
+          atomicOr(d.flags, F_OVERFLOW);
+      }
+      if (stdp) {  // synapseSetLastActiveTime_antiCausalSTDP (DPSNN_neuron_sim.c:179-277)
+        d.last_act[k] = (int32_t)t;
+        int td = (int)t - d.last_spike_ms[j];
+        float a = (td < 128) ? net->anti_tab[td] : 0.0f;
+        d.tderiv[k] = d.tderiv[k] + a;
+      }
+    }
+  }
+  if (lane == 0 && my_events) atomicAdd(d.events, my_events);
+}
+
+// Step 3: the Poisson bath (regularDynamicTimeStep, DPSNN_neuron_sim.c:604-640,
+// getPoissonLapse :844-865).  Each rank owns one serial ran3 stream that its
+// neurons consume in index order.  One block per rank: warp 0 extends the
+// lagged Fibonacci sequence 24 values per round (x[n] = x[n-55] - x[n-24]),
+// all warps turn new draws into the LUT index (uint32)(u*256) and the lapse
+// factor -logf((float)(1-u)), and thread 0 walks the neurons.
+#define BATH_THREADS 256
+#define BATH_CHUNK 1536  // draws generated per refill (multiple of 24)
+
+__device__ static inline float lapse_factor(logf_fixup_t fx, uint32_t mj) {
+  double u = mj * (1.0 / (double)MBIG);
+  double temp = (double)1.0 - u;
+  if (temp < 0) temp = 0;
+  float x = (float)temp;
+  float lf = logf_fixup_lookup(fx, x, logf_cr_from(x, log((double)x)));
+  return -lf;
+}
+
+__global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
+  const NetConst *net = d.net;
+  const uint32_t h = blockIdx.x, t = *d.t;
+  const uint32_t tid = threadIdx.x;
+  __shared__ uint32_t s_hist[64];
+  __shared__ unsigned long long s_produced, s_pos;
+  __shared__ uint32_t s_next_i, s_done, s_out;
+  uint8_t *didx = d.draw_idx + (size_t)h * DRAW_RING;
+  float *dlap = d.draw_lapse + (size_t)h * DRAW_RING;
+  if (tid < 64) s_hist[tid] = d.bath_hist[h * 64 + tid];
+  if (tid == 0) {
+    s_produced = d.bath_produced[h];
+    s_pos = d.bath_pos[h];
+    s_next_i = 0;
+    s_done = 0;
+    s_out = 0;
+  }
+  __syncthreads();
+  const double T0 = (double)t, T1 = (double)(T0 + 1.0);
+  const uint32_t locN = net->locN, i0 = h * locN;
+  const uint64_t ev_base = d.bath_rank_base[h];
+  while (true) {
+    // refill the draw ring ahead of the consumer
+    while ((long long)(s_produced - s_pos) < (long long)net->bath_need) {
+      unsigned long long n0 = s_produced;
+      if (tid < 32) {
+        for (int r = 0; r < BATH_CHUNK / 24; r++) {
+          uint32_t nn = (uint32_t)(n0 + (unsigned long long)r * 24 + tid);
+          int32_t x = 0;
+          if (tid < 24) {
+            x = (int32_t)s_hist[(nn - 55) & 63] - (int32_t)s_hist[(nn - 24) & 63];
+            if (x < 0) x += MBIG;
+          }
+          __syncwarp();
+          if (tid < 24) s_hist[nn & 63] = (uint32_t)x;
+          __syncwarp();
+          if (tid < 24) {
+            // raw draw kept in the lapse slot until all warps convert it
+            dlap[nn & (DRAW_RING - 1)] = __uint_as_float((uint32_t)x);
+          }
+        }
+      }
+      __syncthreads();
+      for (uint32_t k = tid; k < BATH_CHUNK; k += blockDim.x) {
+        uint32_t nn = (uint32_t)(n0 + k) & (DRAW_RING - 1);
+        uint32_t mj = __float_as_uint(dlap[nn]);
+        didx[nn] = (uint8_t)(uint32_t)(mj * (1.0 / (double)MBIG) * 256);
+        dlap[nn] = lapse_factor(d.fix, mj);
+      }
+      __syncthreads();
+      if (tid == 0) s_produced = n0 + BATH_CHUNK;
+      __syncthreads();
+    }
+    if (tid == 0) {
+      unsigned long long pos = s_pos;
+      const unsigned long long lim = s_produced;
+      uint32_t i = s_next_i, out = s_out;
+      while (i < locN) {
+        uint32_t gi = i0 + i;
+        uint32_t mx = d.max_ext[gi];
+        if (lim - pos < 2ull * mx + 8) break;   // refill first
+        double inv = d.inv_nu[gi];
+        double nbv = d.nb[gi];
+        uint32_t c = 0;
+        d.bath_off[gi] = out;
+        if (inv > 0) {
+          if (nbv < T1) {
+            do {
+              d.bath_time[ev_base + out + c] = nbv;
+              d.bath_lut[ev_base + out + c] = didx[pos & (DRAW_RING - 1)];
+              c++;
+              nbv += (double)dlap[(pos + 1) & (DRAW_RING - 1)] * inv;
+              pos += 2;
+            } while ((nbv < T1) && (c < mx));
+            if (c >= mx && nbv < T1) {
+              do {
+                if (pos >= lim) { atomicOr(d.flags, F_BATH_DRAWS); break; }
+                nbv += (double)dlap[pos & (DRAW_RING - 1)] * inv;
+                pos += 1;
+              } while (nbv < T1);
+            }
+          }
+        }
+        d.nb[gi] = nbv;
+        d.bath_cnt[gi] = (uint16_t)c;
+        out += c;
+        i++;
+      }
+      s_next_i = i;
+      s_out = out;
+      s_pos = pos;
+      s_done = (i >= locN);
+    }
+    __syncthreads();
+    if (s_done) break;
+  }
+  if (tid < 64) d.bath_hist[h * 64 + tid] = s_hist[tid];
+  if (tid == 0) {
+    d.bath_produced[h] = s_produced;
+    d.bath_pos[h] = s_pos;
+  }
+}
+
+// LIFCADynamic, non-PerseoDyn branch (DPSNN_neuron_sim.c:664-824).
+struct NeuronRegs {
+  double v, c, tr, te;
+  int fired;
+};
+__device__ static inline void lifca(const NetConst *net, uint32_t s, NeuronRegs &n, double t, double I) {
+  double Tau = net->Tau[s], Theta = net->Theta[s], H = net->H[s], Tarp = net->Tarp[s];
+  double AlphaC = net->AlphaC[s], TauC = net->TauC[s], gC = net->gC[s];
+  double v = n.v, c = n.c, Tr = n.tr, Te = n.te;
+  double deltaT = t - Tr, TFLES = t - Te, rc, TrTe, dth, rmh;
+  if (TFLES > Tarp) {
+    TrTe = Tr - Te;
+    if (TrTe < Tarp) {
+      c *= exp_cr(-(deltaT - TFLES + Tarp) / TauC);
+      deltaT = TFLES - Tarp;
+    }
+    dth = deltaT / 2;
+    rmh = dth / Tau;
+    rc = deltaT / TauC;
+    v = v - v * rmh - gC * c * dth;
+    v = v - v * rmh - gC * c * dth;
+    c = c * (1 - rc + rc * rc / 2);
+    v += I;
+    if (v >= Theta) {
+      v = H;
+      c += AlphaC;
+      Te = t;
+      n.fired = 1;
+    }
+  } else {
+    rc = deltaT / TauC;
+    c = c * (1 - rc + rc * rc / 2);
+  }
+  n.v = v;
+  n.c = c;
+  n.tr = t;
+  n.te = Te;
+}
+
+__device__ static inline double event_time(const Dev &d, uint32_t key, uint32_t t, uint32_t D, uint32_t N) {
+  uint32_t dl = (D - 1) - (key >> 25), q = key & ((1u << 25) - 1);
+  double te = d.ring_te[(size_t)((t + RING_SLOTS - dl) % RING_SLOTS) * N + q];
+  return (double)t + (te - floor(te));   // thisTimeStepF + modf(originalEmissionTime)
+}
+
+// Runs the merged event sequence of one neuron: synaptic events (sorted by
+// (time, key)) merged with the bath events (time-ordered), synaptic first on
+// equal times (mergeFunction, DPSNN_neuron_sim.c:391-421, called at :644-646).
+__device__ static inline void run_neuron(const Dev &d, uint32_t i, uint32_t t, const double *tau,
+                                         const float *val, uint32_t ns) {
+  const NetConst *net = d.net;
+  const uint32_t s = d.sub[i];
+  NeuronRegs n;
+  n.v = d.v[i];
+  n.c = d.c[i];
+  n.tr = d.tr[i];
+  n.te = d.te[i];
+  n.fired = 0;
+  const double T0 = (double)t;
+  const uint32_t boff = d.bath_off[i], bc = d.bath_cnt[i];
+  const uint64_t bbase = d.bath_rank_base[i / net->locN] + boff;
+  const double *lut = d.lut + (size_t)s * 256;
+  uint32_t a = 0, b = 0;
+  double bt = (b < bc) ? d.bath_time[bbase] : 0.0;
+  while (a < ns || b < bc) {
+    double ct, I;
+    if (a < ns && (b >= bc || tau[a] <= bt)) {
+      ct = tau[a];
+      I = (double)val[a];
+      a++;
+    } else {
+      ct = bt;
+      I = lut[d.bath_lut[bbase + b]];
+      b++;
+      if (b < bc) bt = d.bath_time[bbase + b];
+    }
+    if (((ct - T0) >= 1.0) || ((ct - T0) < 0)) atomicOr(d.flags, F_TIME_WINDOW);
+    lifca(net, s, n, ct, I);
+  }
+  d.v[i] = n.v;
+  d.c[i] = n.c;
+  d.tr[i] = n.tr;
+  d.te[i] = n.te;
+  if (n.fired) d.fired[i] = 1;
+}
+
+// Step 4: neuron update, one thread per neuron (regularDynamicTimeStep,
+// DPSNN_neuron_sim.c:522-662).  Neurons with more events than the thread
+// buffer holds are queued for heavy_kernel.
+__global__ void __launch_bounds__(NEURON_BLOCK) neuron_kernel(Dev d) {
+  const NetConst *net = d.net;
+  const uint32_t t = *d.t, N = net->N, D = net->D, cap = net->ev_cap;
+  const uint32_t i = blockIdx.x * NEURON_BLOCK + threadIdx.x;
+  int fired = 0;
+  if (i < N) {
+    uint32_t cnt = d.ev_cnt[i];
+    d.ev_cnt[i] = 0;
+    if (cnt > cap || cnt > LOCAL_EVENTS) {
+      uint32_t k = atomicAdd(d.heavy_cnt, 1u);
+      if (k < N) {
+        d.heavy_list[k] = i;
+        d.heavy_list[N + k] = cnt;
+      }
+    } else {
+      double tau[LOCAL_EVENTS];
+      float val[LOCAL_EVENTS];
+      uint32_t key[LOCAL_EVENTS];
+      const uint2 *ev = d.ev + (size_t)i * cap;
+      for (uint32_t e = 0; e < cnt; e++) {
+        uint2 x = ev[e];
+        double tm = event_time(d, x.x, t, D, N);
+        // stable insertion by (time, key)
+        uint32_t p = e;
+        while (p > 0 && (tau[p - 1] > tm || (tau[p - 1] == tm && key[p - 1] > x.x))) {
+          tau[p] = tau[p - 1];
+          val[p] = val[p - 1];
+          key[p] = key[p - 1];
+          p--;
+        }
+        tau[p] = tm;
+        val[p] = __uint_as_float(x.y);
+        key[p] = x.x;
+      }
+      run_neuron(d, i, t, tau, val, cnt);
+      fired = d.fired[i];
+    }
+  }
+  uint32_t bc = __syncthreads_count(fired);
+  if (threadIdx.x == 0) d.block_fired[blockIdx.x] = bc;
+}
+
+// Neurons with many events in one step: gather bucket + overflow events into
+// global scratch, sort by (time, key), run.  The last block also advances
+// the step counter.
+__global__ void heavy_kernel(Dev d) {
+  const NetConst *net = d.net;
+  const uint32_t t = *d.t, N = net->N, D = net->D, cap = net->ev_cap;
+  const uint32_t nh = min(*d.heavy_cnt, N);
+  const uint32_t novf = min(*d.ovf_cnt, net->ovf_cap);
+  for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < nh; h += gridDim.x * blockDim.x) {
+    uint32_t i = d.heavy_list[h], cnt = d.heavy_list[N + h];
+    if (cnt > MAX_INPUTS_PER_STEP) {
+      atomicOr(d.flags, F_TOO_MANY_INPUTS);
+      continue;
+    }
+    unsigned long long off = atomicAdd((unsigned long long *)d.heavy_scratch_used, (unsigned long long)cnt);
+    if (off + cnt > d.heavy_scratch_cap) {
+      atomicOr(d.flags, F_OVERFLOW);
+      continue;
+    }
+    uint2 *ks = d.heavy_scratch + off;
+    double *ts = d.heavy_tau + off;
+    uint32_t k = 0;
+    for (uint32_t e = 0; e < min(cnt, cap); e++) ks[k++] = d.ev[(size_t)i * cap + e];
+    for (uint32_t o = 0; o < novf && k < cnt; o++) {
+      uint4 x = d.ovf[o];
+      if (x.x == i) ks[k++] = make_uint2(x.y, x.z);
+    }
+    for (uint32_t e = 0; e < k; e++) {
+      uint2 x = ks[e];
+      double tm = event_time(d, x.x, t, D, N);
+      uint32_t p = e;
+      while (p > 0 && (ts[p - 1] > tm || (ts[p - 1] == tm && ks[p - 1].x > x.x))) {
+        ts[p] = ts[p - 1];
+        ks[p] = ks[p - 1];
+        p--;
+      }
+      ts[p] = tm;
+      ks[p] = x;
+    }
+    // run_neuron takes separate value array: reuse the key slots' y halves
+    float *vals = (float *)(d.heavy_tau + d.heavy_scratch_cap) + off;
+    for (uint32_t e = 0; e < k; e++) vals[e] = __uint_as_float(ks[e].y);
+    run_neuron(d, i, t, ts, vals, k);
+    if (d.fired[i]) atomicAdd(&d.block_fired[i / NEURON_BLOCK], 1u);
+  }
+}
+
+// Long term plasticity at x999 ms (longTermPlasticity, DPSNN_localNet_sim.c:312-414),
+// one warp per presynaptic neuron.
+__global__ void ltp_kernel(Dev d) {
+  const NetConst *net = d.net;
+  const uint32_t t = *d.t;
+  if (!((t % 1000) == 999 && t >= net->start_pl && t <= net->stop_pl)) return;
+  const uint32_t N = net->N, lane = threadIdx.x & 31;
+  for (uint32_t P = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; P < N;
+       P += (gridDim.x * blockDim.x) >> 5) {
+    uint32_t sp = d.sub[P];
+    for (uint64_t k = d.row_ptr[P] + lane; k < d.row_ptr[P + 1]; k += 32) {
+      uint32_t tp = d.sub[d.post[k]];
+      float maxv = (float)(2.0 * net->J[sp * DPSNN_MAX_SUBPOP + tp]);
+      float rmaxv = (float)(2.0 * net->J[tp * DPSNN_MAX_SUBPOP + sp]);
+      float clamp = 0.0f;
+      float td = d.tderiv[k];
+      if (maxv > 0.0 && rmaxv > 0.0) {
+        float wF = (float)(d.w16[k] * net->w2f);
+        float dF = td;
+        dF += net->stdp_drift;
+        wF = wF + dF;
+        if (wF > maxv) { clamp = (wF - maxv); dF = dF - clamp; wF = maxv; }
+        if (wF < 0.0) { clamp = wF; dF = dF - clamp; wF = 0.0f; }
+        d.w16[k] = (int16_t)(wF * net->f2w);
+        td = dF;
+      }
+      if (net->stdp_tauDecay == 1.0f)
+        td = 0.0f;
+      else
+        td = (td - net->stdp_drift + clamp) * (1 - 1 / net->stdp_tauDecay);
+      d.tderiv[k] = td;
+    }
+  }
+}
+
+__global__ void end_step_kernel(Dev d) {
+  *d.ovf_cnt = 0;
+  *d.heavy_cnt = 0;
+  *d.heavy_scratch_used = 0;
+  *d.t = *d.t + 1;
+}
+
+// Per-(neuron, delay) counts of the chosen hypothesis -> per-row totals and
+// the in-row per-delay offsets.
+__global__ void counts_to_csr_kernel(const NetConst *net, const uint16_t *cnt_out,
+                                     const int32_t *hyp, uint16_t *sub_off, uint32_t *row_len) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= net->N) return;
+  uint32_t D = net->D;
+  int h = hyp[i / net->npcm];
+  const uint16_t *c = cnt_out + ((size_t)h * net->N + i) * D;
+  uint32_t acc = 0;
+  for (uint32_t dl = 0; dl < D; dl++) {
+    sub_off[(size_t)i * (D + 1) + dl] = (uint16_t)acc;
+    acc += c[dl];
+  }
+  sub_off[(size_t)i * (D + 1) + D] = (uint16_t)acc;
+  row_len[i] = acc;
+}
+
+__global__ void init_neurons_kernel(Dev d) {
+  const NetConst *net = d.net;
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= net->N) return;
+  // initNeuralKind (DPSNN_neuron_init.c:99-115); Tr is zero (static storage)
+  d.v[i] = net->H[d.sub[i]];
+  d.c[i] = 0.0;
+  d.te[i] = -1000;
+  d.nb[i] = 0.0;
+  d.tr[i] = 0.0;
+  d.fired[i] = 0;
+  d.last_spike_ms[i] = -100000;  // DPSNN_localNet_init.c:217
+  d.ev_cnt[i] = 0;
+}
+
+// incoming-synapse lists (causal STDP), per post neuron
+__global__ void in_count_kernel(const NetConst *net, const uint32_t *post, uint64_t S, uint64_t *in_ptr) {
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < S; k += (uint64_t)gridDim.x * blockDim.x)
+    atomicAdd((unsigned long long *)&in_ptr[post[k] + 1], 1ull);
+}
+__global__ void in_fill_kernel(const NetConst *net, const uint32_t *post, uint64_t S, const uint64_t *in_ptr,
+                               unsigned long long *fill, uint32_t *in_idx) {
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < S; k += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t j = post[k];
+    unsigned long long p = atomicAdd(&fill[j], 1ull);
+    in_idx[in_ptr[j] + p] = (uint32_t)k;
+  }
+}
+
+// per (rank, delay): max and min presynaptic index among synapses aimed at
+// that rank -- used to detect the reference's run-over-group-end search case
+__global__ void group_extrema_kernel(const NetConst *net, const uint64_t *row_ptr, const uint16_t *sub_off,
+                                     const uint32_t *post, uint32_t *gmax, uint32_t *gmin) {
+  const uint32_t N = net->N, D = net->D, lane = threadIdx.x & 31;
+  for (uint32_t P = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; P < N; P += (gridDim.x * blockDim.x) >> 5) {
+    for (uint32_t dl = 0; dl < D; dl++) {
+      uint64_t b = row_ptr[P] + sub_off[(size_t)P * (D + 1) + dl], e = row_ptr[P] + sub_off[(size_t)P * (D + 1) + dl + 1];
+      for (uint64_t k = b + lane; k < e; k += 32) {
+        uint32_t h = post[k] / net->locN;
+        atomicMax(&gmax[h * D + dl], P);
+        atomicMin(&gmin[h * D + dl], P);
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ host engine
+struct dpsnn_engine {
+  NetConst hnet;
+  Dev d;
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  uint64_t S = 0;
+  uint32_t t_host = 0;   // steps enqueued
+  std::vector<void *> allocs;
+  uint32_t grid_neuron = 0, grid_deliver = 0;
+  int timing = 0;
+  cudaEvent_t ev[12];
+  double ktime[5] = {0, 0, 0, 0, 0};
+  uint64_t klaunch[5] = {0, 0, 0, 0, 0};
+  std::vector<float> fix_vals;
+  std::vector<uint32_t> fix_keys, fix_bucket;
+};
+
+template <typename T>
+static int dalloc(dpsnn_engine *e, T **p, size_t n, bool zero = true) {
+  void *q = nullptr;
+  size_t bytes = std::max<size_t>(n * sizeof(T), 16);
+  cudaError_t err = cudaMalloc(&q, bytes);
+  if (err != cudaSuccess)
+    return dpsnn_fail(DPSNN_E_NOMEM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(err));
+  e->allocs.push_back(q);
+  if (zero) {
+    err = cudaMemsetAsync(q, 0, bytes, e->stream);
+    if (err != cudaSuccess) return dpsnn_fail(DPSNN_E_CUDA, "cudaMemset: %s", cudaGetErrorString(err));
+  }
+  *p = (T *)q;
+  return 0;
+}
+#define DALLOC(ptr, n)                          \
+  do {                                          \
+    int rc_ = dalloc(e, &(ptr), (size_t)(n));   \
+    if (rc_) return rc_;                        \
+  } while (0)
+
+static int load_logf_fixup(dpsnn_engine *e) {
+  std::string path = std::string(dpsnn_library_dir()) + "/logf_fixup.bin";
+  const char *envp = getenv("DPSNN_LOGF_FIXUP");
+  if (envp) path = envp;
+  FILE *f = fopen(path.c_str(), "rb");
+  if (!f) return dpsnn_fail(DPSNN_E_PARAM, "cannot open %s (built with the engine)", path.c_str());
+  uint32_t n = 0;
+  bool ok = fread(&n, 4, 1, f) == 1;
+  e->fix_keys.resize(n);
+  e->fix_vals.resize(n);
+  e->fix_bucket.resize(LOGF_FIX_NBUCKET);
+  ok = ok && fread(e->fix_keys.data(), 4, n, f) == n;
+  ok = ok && fread(e->fix_vals.data(), 4, n, f) == n;
+  ok = ok && fread(e->fix_bucket.data(), 4, LOGF_FIX_NBUCKET, f) == LOGF_FIX_NBUCKET;
+  fclose(f);
+  if (!ok) return dpsnn_fail(DPSNN_E_PARAM, "truncated %s", path.c_str());
+  uint32_t *k; float *v; uint32_t *b;
+  DALLOC(k, n);
+  DALLOC(v, n);
+  DALLOC(b, LOGF_FIX_NBUCKET);
+  CK(cudaMemcpyAsync(k, e->fix_keys.data(), 4ull * n, cudaMemcpyHostToDevice, e->stream));
+  CK(cudaMemcpyAsync(v, e->fix_vals.data(), 4ull * n, cudaMemcpyHostToDevice, e->stream));
+  CK(cudaMemcpyAsync(b, e->fix_bucket.data(), 4ull * LOGF_FIX_NBUCKET, cudaMemcpyHostToDevice, e->stream));
+  e->d.fix.keys = k;
+  e->d.fix.vals = v;
+  e->d.fix.bucket = b;
+  e->d.fix.n = n;
+  return 0;
+}
+
+// ---- erflib Gaussian LUT on the host (erflib.c:41-169), C library exp
+static double h_erfcc(double x) {
+  double t, z, ans;
+  z = fabs(x);
+  t = 1.0 / (1.0 + 0.5 * z);
+  ans = t * exp(-z * z - 1.26551223 +
+                t * (1.00002368 +
+                     t * (0.37409196 +
+                          t * (0.09678418 +
+                               t * (-0.18628806 +
+                                    t * (0.27886807 +
+                                         t * (-1.13520398 +
+                                              t * (1.48851587 + t * (-0.82215223 + t * 0.17087277)))))))));
+  return x >= 0.0 ? ans : 2.0 - ans;
+}
+static double h_normcum(double x, double mu, double sigma) {
+  return 1 - 0.5 * h_erfcc((x - mu) / (sqrt(2.0) * sigma));
+}
+static double h_cutnormcum(double x, double mu, double sigma, double a, double b) {
+  double n0 = h_normcum(a, mu, sigma);
+  return (h_normcum(x, mu, sigma) - n0) / (h_normcum(b, mu, sigma) - n0);
+}
+static double h_findprob(double p, double mu, double sigma, double a, double b) {
+  double err = 1e-6, x, xmin = a, xmax = b;
+  int maxit = 256, i = 0;
+  if (p <= 0.0) return a;
+  if (p >= 1.0) return b;
+  while ((xmax - xmin) > err && i < maxit) {
+    x = (xmax + xmin) * 0.5;
+    if (h_cutnormcum(x, mu, sigma, a, b) < p)
+      xmin = x;
+    else
+      xmax = x;
+    i++;
+  }
+  return (xmax + xmin) * 0.5;
+}
+static void h_gaussian_lut(double mu, double sigma, double xmin, double xmax, double *table) {
+  if (sigma > 0.0) {
+    double dp = 1.0 / 256.0, x0, x1 = xmin, p;
+    int i;
+    for (p = dp, i = 0; p <= 1.0; p += dp, i++) {
+      x0 = x1;
+      x1 = h_findprob(p, mu, sigma, xmin, xmax);
+      table[i] = (x1 + x0) * 0.5;
+    }
+  } else {
+    for (int i = 0; i < 256; i++) table[i] = mu;
+  }
+}
+
+static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_options *o) {
+  NetConst &n = e->hnet;
+  memset(&n, 0, sizeof n);
+  if (p->nsub == 0 || p->nsub > DPSNN_MAX_SUBPOP)
+    return dpsnn_fail(DPSNN_E_PARAM, "number of sub-populations %u out of range", p->nsub);
+  if (p->stencil_dim == 0 || !p->spec || !p->bath) return dpsnn_fail(DPSNN_E_PARAM, "missing stencil description");
+  if (p->D == 0 || p->D > RING_SLOTS) return dpsnn_fail(DPSNN_E_PARAM, "env_D=%u out of range [1,%d]", p->D, RING_SLOTS);
+  if (p->glob_h == 0) return dpsnn_fail(DPSNN_E_PARAM, "env_globH must be >= 1");
+  n.nsub = p->nsub;
+  n.npcm = 0;
+  for (uint32_t s = 0; s < n.nsub; s++) {
+    n.offset[s] = n.npcm;
+    n.count[s] = p->count[s];
+    n.npcm += p->count[s];
+  }
+  if (n.npcm == 0) return dpsnn_fail(DPSNN_E_PARAM, "neuronsPerCM <= 0");
+  n.cfx = p->cfx;
+  n.cfy = p->cfy;
+  n.nmod = p->cfx * p->cfy;
+  if (n.nmod == 0) return dpsnn_fail(DPSNN_E_PARAM, "empty grid");
+  if ((n.nmod % p->glob_h) != 0 || p->glob_h > n.nmod)
+    return dpsnn_fail(DPSNN_E_PARAM, "#processes and #cort. columns must be multiple OR equal");
+  n.P = p->glob_h;
+  n.mods_per_rank = n.nmod / n.P;
+  n.locN = n.npcm * n.mods_per_rank;
+  n.N = n.locN * n.P;
+  if ((uint64_t)n.npcm * n.nmod >= (1ull << 25))
+    return dpsnn_fail(DPSNN_E_PARAM, "network of %llu neurons exceeds the engine limit of 2^25",
+                      (unsigned long long)n.npcm * n.nmod);
+  n.D = p->D;
+  n.stencil_dim = p->stencil_dim;
+  n.max_mod = p->stencil_dim - 1;
+  n.stencil = 2 * p->stencil_dim - 1;
+  for (uint32_t s = 0; s < n.nsub; s++) {
+    n.Tau[s] = p->Tau[s];
+    n.Theta[s] = p->Theta[s];
+    n.H[s] = p->H[s];
+    n.Tarp[s] = p->Tarp[s];
+    n.AlphaC[s] = p->AlphaC[s];
+    n.TauC[s] = p->TauC[s];
+    n.gC[s] = p->gC[s];
+    n.NuExt[s] = p->NuExt[s];
+    for (uint32_t t = 0; t < n.nsub; t++) {
+      n.J[s * DPSNN_MAX_SUBPOP + t] = p->J[s * p->nsub + t];
+      n.DJ[s * DPSNN_MAX_SUBPOP + t] = p->DJ[s * p->nsub + t];
+      n.DMin[s * DPSNN_MAX_SUBPOP + t] = p->DMin[s * p->nsub + t];
+      n.DMax[s * DPSNN_MAX_SUBPOP + t] = p->DMax[s * p->nsub + t];
+    }
+  }
+  {
+    double dmin = 1e36, dmax = 0;
+    for (uint32_t s = 0; s < n.nsub; s++)
+      for (uint32_t t = 0; t < n.nsub; t++) {
+        if (n.DMax[s * DPSNN_MAX_SUBPOP + t] > dmax) dmax = n.DMax[s * DPSNN_MAX_SUBPOP + t];
+        if (n.DMin[s * DPSNN_MAX_SUBPOP + t] < dmin) dmin = n.DMin[s * DPSNN_MAX_SUBPOP + t];
+      }
+    n.delay_min = (uint32_t)dmin;
+    n.delay_max = (uint32_t)dmax;
+  }
+  if (!(p->min_syn_weight_f < 0) || p->min_syn_weight_f < -6.0f)
+    return dpsnn_fail(DPSNN_E_PARAM, "env_minSynWeigth out of range -6.000000 - 0.0");
+  n.f2w = -32767 / p->min_syn_weight_f;
+  n.w2f = p->min_syn_weight_f / -32767;
+  n.min_w = p->min_syn_weight_f;
+  n.global_seed = p->global_seed;
+  n.start_pl = p->start_plasticity_ms;
+  n.stop_pl = p->stop_plasticity_ms;
+  n.stdp_on = (p->start_plasticity_ms <= p->stop_plasticity_ms &&
+               p->start_plasticity_ms < (p->total_sim_time_ms ? p->total_sim_time_ms : 0xFFFFFFFFu)) ? 1 : 0;
+  n.causal_tab[0] = p->stdp_causalMax * p->stdp_multiplier;
+  n.causal_tab[1] = n.causal_tab[0];
+  n.anti_tab[0] = p->stdp_antiCausalCoeff * p->stdp_antiCausalMax * p->stdp_multiplier;
+  for (int i = 1; i < 128; i++) n.causal_tab[i] = (1 - 1 / p->stdp_tau_ms) * n.causal_tab[i - 1];
+  for (int i = 1; i < 128; i++) n.anti_tab[i] = (1 - 1 / p->stdp_tau_ms) * n.anti_tab[i - 1];
+  n.stdp_drift = p->stdp_drift;
+  n.stdp_tauDecay = p->stdp_tauDecay_s;
+  n.ev_cap = (o && o->events_per_neuron) ? o->events_per_neuron : LOCAL_EVENTS;
+  if (n.ev_cap > LOCAL_EVENTS) n.ev_cap = LOCAL_EVENTS;
+  n.ovf_cap = (o && o->overflow_events) ? o->overflow_events : (1u << 22);
+
+  Dev &d = e->d;
+  const uint32_t N = n.N, D = n.D, P = n.P;
+  DALLOC(d.net, 1);
+  CK(cudaMemcpyAsync(d.net, &n, sizeof n, cudaMemcpyHostToDevice, e->stream));
+  // bath LUTs (initLUT, DPSNN_LIFCAcorticalModuleGen.cpp:347-356)
+  {
+    std::vector<double> lut((size_t)n.nsub * 256);
+    for (uint32_t s = 0; s < n.nsub; s++) {
+      float J = p->JExt[s], DJ = p->DJExt[s];
+      h_gaussian_lut(J, J * DJ, 0.0, 2.0 * J, &lut[(size_t)s * 256]);
+    }
+    DALLOC(d.lut, lut.size());
+    CK(cudaMemcpyAsync(d.lut, lut.data(), lut.size() * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+  }
+  // mirrored stencil probabilities (initProbConnectMatrix, LIFCAconnectome.cpp:136-198)
+  float *dprob;
+  {
+    const uint32_t st = n.stencil, M = n.max_mod, S = p->stencil_dim;
+    std::vector<float> prob((size_t)DPSNN_MAX_SUBPOP * DPSNN_MAX_SUBPOP * st * st, 0.0f);
+    for (uint32_t s = 0; s < n.nsub; s++)
+      for (uint32_t t = 0; t < n.nsub; t++)
+        for (uint32_t x = 0; x <= M; x++)
+          for (uint32_t y = 0; y <= M; y++) {
+            float v = p->spec[((size_t)(s * n.nsub + t) * S + x) * S + y];
+            auto at = [&](uint32_t X, uint32_t Y) -> float & {
+              return prob[(((size_t)s * DPSNN_MAX_SUBPOP + t) * st + X) * st + Y];
+            };
+            at(M + x, M + y) = v;
+            at(M - x, M + y) = v;
+            at(M - x, M - y) = v;
+            at(M + x, M - y) = v;
+          }
+    DALLOC(dprob, prob.size());
+    CK(cudaMemcpyAsync(dprob, prob.data(), prob.size() * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+  }
+  // neuron arrays
+  DALLOC(d.v, N); DALLOC(d.c, N); DALLOC(d.tr, N); DALLOC(d.te, N); DALLOC(d.nb, N);
+  DALLOC(d.inv_nu, N); DALLOC(d.max_ext, N); DALLOC(d.sub, N); DALLOC(d.fired, N);
+  DALLOC(d.last_spike_ms, N);
+  e->grid_neuron = (N + NEURON_BLOCK - 1) / NEURON_BLOCK;
+  DALLOC(d.block_fired, e->grid_neuron);
+
+  // ---- synapse generation, pass A (both NormDev-cache hypotheses)
+  const uint32_t nmod = n.nmod;
+  GenRecord *drec;
+  uint16_t *cnt_out;
+  uint32_t *scratch;
+  DALLOC(drec, 2 * nmod);
+  DALLOC(cnt_out, 2ull * N * D);
+  const uint32_t SD = p->stencil_dim;
+  uint32_t *bath_tmpl;
+  {
+    DALLOC(scratch, (size_t)2 * nmod * MAX_SYN_PER_NEURON);
+    DALLOC(bath_tmpl, SD * SD);
+    std::vector<uint32_t> bath(p->bath, p->bath + SD * SD);
+    CK(cudaMemcpyAsync(bath_tmpl, bath.data(), 4ull * SD * SD, cudaMemcpyHostToDevice, e->stream));
+  }
+  int32_t *dhyp;
+  double *dcache;
+  DALLOC(dhyp, nmod);
+  DALLOC(dcache, nmod);
+  gen_kernel<<<(2 * nmod + 63) / 64, 64, 0, e->stream>>>(d.net, dprob, 0, drec, dhyp, dcache, cnt_out,
+                                                          nullptr, nullptr, nullptr, nullptr, scratch,
+                                                          bath_tmpl, nullptr, nullptr, nullptr);
+  CK(cudaGetLastError());
+  std::vector<GenRecord> rec(2 * nmod);
+  CK(cudaMemcpyAsync(rec.data(), drec, sizeof(GenRecord) * 2 * nmod, cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  for (uint32_t k = 0; k < 2 * nmod; k++)
+    if (rec[k].err && !((k & 1) && (k / 2) % n.mods_per_rank == 0)) {
+      const char *what[] = {"", "too many synapses generated for neuron", "synaptic weight out of minSynWeight_f range",
+                            "connection probability in (0,1e-5] is not supported", "delay >= env_D",
+                            "zero mean synaptic efficacy"};
+      return dpsnn_fail(DPSNN_E_MODEL, "synapse generation: %s (%u)", what[rec[k].err], rec[k].err_arg);
+    }
+  // resolve the NormDev cache hand-off rank by rank, module by module
+  std::vector<int32_t> hyp(nmod);
+  std::vector<double> cache(nmod, 0.0);
+  for (uint32_t h = 0; h < P; h++) {
+    int32_t set = 0;
+    double cval = 0.0;
+    for (uint32_t mm = 0; mm < n.mods_per_rank; mm++) {
+      uint32_t m = h * n.mods_per_rank + mm;
+      int choose = 0;
+      if (mm > 0 && set == 1) {
+        const GenRecord &r1 = rec[2 * m + 1];
+        if (!r1.used_normdev) {
+          choose = 1;
+        } else {
+          float mean = r1.first_mean, sigma = r1.first_sigma;
+          float wf = (float)(mean + cval * sigma);
+          bool acc = (mean > 0.0) ? !((wf < 0.0) || (wf >= 2.0 * mean)) : !((wf <= 2.0 * mean) || (wf > 0));
+          choose = acc ? 1 : 0;
+        }
+      }
+      hyp[m] = choose;
+      cache[m] = cval;
+      const GenRecord &rc = rec[2 * m + choose];
+      if (rc.used_normdev) {
+        set = rc.set_out;
+        cval = rc.cache_out;
+      }
+    }
+  }
+  CK(cudaMemcpyAsync(dhyp, hyp.data(), 4ull * nmod, cudaMemcpyHostToDevice, e->stream));
+  CK(cudaMemcpyAsync(dcache, cache.data(), 8ull * nmod, cudaMemcpyHostToDevice, e->stream));
+  // ---- CSR offsets from the chosen counts
+  uint32_t *row_len;
+  DALLOC(d.sub_off, (size_t)N * (D + 1));
+  DALLOC(row_len, N);
+  counts_to_csr_kernel<<<(N + 255) / 256, 256, 0, e->stream>>>(d.net, cnt_out, dhyp, d.sub_off, row_len);
+  CK(cudaGetLastError());
+  std::vector<uint32_t> hlen(N);
+  std::vector<uint64_t> hrow(N + 1);
+  CK(cudaMemcpyAsync(hlen.data(), row_len, 4ull * N, cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  hrow[0] = 0;
+  for (uint32_t i = 0; i < N; i++) hrow[i + 1] = hrow[i] + hlen[i];
+  e->S = hrow[N];
+  DALLOC(d.row_ptr, N + 1);
+  CK(cudaMemcpyAsync(d.row_ptr, hrow.data(), 8ull * (N + 1), cudaMemcpyHostToDevice, e->stream));
+  DALLOC(d.post, e->S);
+  DALLOC(d.w16, e->S);
+  // ---- pass B: regenerate the chosen hypothesis straight into the CSR
+  gen_kernel<<<(nmod + 63) / 64, 64, 0, e->stream>>>(d.net, dprob, 1, drec, dhyp, dcache, cnt_out, d.row_ptr,
+                                                      d.sub_off, d.post, d.w16, scratch, bath_tmpl, d.inv_nu,
+                                                      d.max_ext, d.sub);
+  CK(cudaGetLastError());
+  std::vector<GenRecord> recB(nmod);
+  CK(cudaMemcpyAsync(recB.data(), drec, sizeof(GenRecord) * nmod, cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  for (uint32_t m = 0; m < nmod; m++)
+    if (recB[m].err) return dpsnn_fail(DPSNN_E_MODEL, "synapse generation pass B error %d", recB[m].err);
+  // free generation scratch
+  for (void *q : {(void *)cnt_out, (void *)scratch, (void *)row_len, (void *)bath_tmpl}) {
+    cudaFree(q);
+    e->allocs.erase(std::find(e->allocs.begin(), e->allocs.end(), q));
+  }
+  // ---- run-over-group-end check (see DPSNN_synapse.c:211-265): the reference's
+  // search continues past a (delay, source rank) group while the next entry has
+  // the same presynaptic index; this happens only when the last source of a
+  // delay group is also the first source of the next non-empty group.
+  {
+    uint32_t *gmax, *gmin;
+    DALLOC(gmax, (size_t)P * D);
+    DALLOC(gmin, (size_t)P * D);
+    CK(cudaMemsetAsync(gmin, 0xFF, 4ull * P * D, e->stream));
+    group_extrema_kernel<<<std::min<uint32_t>(4096, (N + 7) / 8), 256, 0, e->stream>>>(d.net, d.row_ptr,
+                                                                                     d.sub_off, d.post, gmax, gmin);
+    CK(cudaGetLastError());
+    std::vector<uint32_t> hmax((size_t)P * D), hmin((size_t)P * D);
+    CK(cudaMemcpyAsync(hmax.data(), gmax, 4ull * P * D, cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaMemcpyAsync(hmin.data(), gmin, 4ull * P * D, cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    for (uint32_t h = 0; h < P; h++)
+      for (uint32_t dl = 0; dl < D; dl++) {
+        if (hmin[h * D + dl] == 0xFFFFFFFFu) continue;
+        uint32_t dn = dl + 1;
+        while (dn < D && hmin[h * D + dn] == 0xFFFFFFFFu) dn++;
+        if (dn < D && hmax[h * D + dl] == hmin[h * D + dn])
+          return dpsnn_fail(DPSNN_E_MODEL,
+                            "rank %u: neuron %u ends delay group %u and starts group %u; the reference's "
+                            "search would run across the group boundary (not reproduced)",
+                            h, hmax[h * D + dl], dl, dn);
+      }
+  }
+  // ---- STDP arrays
+  if (n.stdp_on) {
+    DALLOC(d.tderiv, e->S);
+    DALLOC(d.last_act, e->S);
+    DALLOC(d.in_ptr, N + 1);
+    DALLOC(d.in_idx, e->S);
+    unsigned long long *fill;
+    DALLOC(fill, N);
+    in_count_kernel<<<2048, 256, 0, e->stream>>>(d.net, d.post, e->S, d.in_ptr);
+    CK(cudaGetLastError());
+    std::vector<uint64_t> ip(N + 1);
+    CK(cudaMemcpyAsync(ip.data(), d.in_ptr, 8ull * (N + 1), cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    for (uint32_t i = 0; i < N; i++) {
+      if (ip[i + 1] >= 2 * MAX_SYN_PER_NEURON)
+        return dpsnn_fail(DPSNN_E_MODEL, "ERROR too many syn incoming on neuron glob_n=%u", i);
+      ip[i + 1] += ip[i];
+    }
+    CK(cudaMemcpyAsync(d.in_ptr, ip.data(), 8ull * (N + 1), cudaMemcpyHostToDevice, e->stream));
+    in_fill_kernel<<<2048, 256, 0, e->stream>>>(d.net, d.post, e->S, d.in_ptr, fill, d.in_idx);
+    CK(cudaGetLastError());
+  }
+  // ---- ring, events, bath
+  DALLOC(d.ring_ids, (size_t)RING_SLOTS * N);
+  DALLOC(d.ring_te, (size_t)RING_SLOTS * N);
+  DALLOC(d.ring_cnt, RING_SLOTS);
+  DALLOC(d.ev_cnt, N);
+  DALLOC(d.ev, (size_t)N * n.ev_cap);
+  DALLOC(d.ovf_cnt, 1);
+  DALLOC(d.ovf, n.ovf_cap);
+  DALLOC(d.heavy_list, 2ull * N);
+  DALLOC(d.heavy_cnt, 1);
+  d.heavy_scratch_cap = (uint64_t)n.ovf_cap + 64ull * MAX_INPUTS_PER_STEP;
+  DALLOC(d.heavy_scratch, d.heavy_scratch_cap);
+  DALLOC(d.heavy_tau, d.heavy_scratch_cap * 2);   // times, then float values
+  DALLOC(d.heavy_scratch_used, 2);
+  DALLOC(d.t, 1);
+  DALLOC(d.flags, 4);
+  DALLOC(d.events, 1);
+  init_neurons_kernel<<<(N + 255) / 256, 256, 0, e->stream>>>(d);
+  CK(cudaGetLastError());
+  {
+    // per-rank bath event capacity = sum of maxExternCurrentCount
+    std::vector<uint32_t> mx(N);
+    CK(cudaMemcpyAsync(mx.data(), d.max_ext, 4ull * N, cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    std::vector<uint64_t> base(P + 1, 0);
+    for (uint32_t h = 0; h < P; h++) {
+      uint64_t s = 0;
+      for (uint32_t i = h * n.locN; i < (h + 1) * n.locN; i++) s += mx[i];
+      base[h + 1] = base[h] + s;
+    }
+    uint32_t mx_max = 0;
+    for (uint32_t i = 0; i < N; i++) mx_max = std::max(mx_max, mx[i]);
+    if (mx_max > 8192)
+      return dpsnn_fail(DPSNN_E_CAPACITY, "maxExternCurrentCount %u exceeds the bath buffer (8192)", mx_max);
+    n.bath_need = 2 * BATH_CHUNK + 2 * mx_max + 16;
+    CK(cudaMemcpyAsync(d.net, &n, sizeof n, cudaMemcpyHostToDevice, e->stream));
+    DALLOC(d.bath_rank_base, P + 1);
+    CK(cudaMemcpyAsync(d.bath_rank_base, base.data(), 8ull * (P + 1), cudaMemcpyHostToDevice, e->stream));
+    DALLOC(d.bath_time, base[P]);
+    DALLOC(d.bath_lut, base[P]);
+    DALLOC(d.bath_off, N);
+    DALLOC(d.bath_cnt, N);
+    // dynamics streams: SetRandomSeed(loc_h) (DPSNN_localNet_init.c:283).
+    // Rank 0 continues its generation stream; others re-initialise.
+    std::vector<uint32_t> hist((size_t)P * 64, 0);
+    std::vector<uint64_t> produced(P, 0), pos(P, 1);
+    for (uint32_t h = 0; h < P; h++) {
+      uint32_t h55[55];
+      if (h == 0) {
+        memcpy(h55, recB[n.mods_per_rank - 1].hist, sizeof h55);
+      } else {
+        Ran3 g;
+        memset(&g, 0, sizeof g);
+        g.idum = -(int32_t)h;
+        // table initialisation only; the draw SetRandomSeed makes is x[0]
+        int32_t mj = MSEED - (int32_t)h, mk;
+        mj = (mj < 0 ? -mj : mj) % MBIG;
+        g.ma[55] = mj;
+        mk = 1;
+        for (int i = 1; i <= 54; i++) {
+          int ii = (21 * i) % 55;
+          g.ma[ii] = mk;
+          mk = mj - mk;
+          if (mk < 0) mk += MBIG;
+          mj = g.ma[ii];
+        }
+        for (int k = 1; k <= 4; k++)
+          for (int i = 1; i <= 55; i++) {
+            g.ma[i] -= g.ma[1 + (i + 30) % 55];
+            if (g.ma[i] < 0) g.ma[i] += MBIG;
+          }
+        g.inext = 0;
+        r3_history(g, h55);
+      }
+      // x[-55..-1] at ring positions (k-55) & 63
+      for (int k = 0; k < 55; k++) hist[(size_t)h * 64 + ((k - 55) & 63)] = h55[k];
+    }
+    DALLOC(d.bath_hist, (size_t)P * 64);
+    DALLOC(d.bath_produced, P);
+    DALLOC(d.bath_pos, P);
+    DALLOC(d.draw_idx, (size_t)P * DRAW_RING);
+    DALLOC(d.draw_lapse, (size_t)P * DRAW_RING);
+    CK(cudaMemcpyAsync(d.bath_hist, hist.data(), 4ull * P * 64, cudaMemcpyHostToDevice, e->stream));
+    CK(cudaMemcpyAsync(d.bath_produced, produced.data(), 8ull * P, cudaMemcpyHostToDevice, e->stream));
+    CK(cudaMemcpyAsync(d.bath_pos, pos.data(), 8ull * P, cudaMemcpyHostToDevice, e->stream));
+  }
+  int rc = load_logf_fixup(e);
+  if (rc) return rc;
+  cudaFree(dprob);
+  e->allocs.erase(std::find(e->allocs.begin(), e->allocs.end(), (void *)dprob));
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
+  e->grid_deliver = (uint32_t)sms * 8;
+  CK(cudaStreamSynchronize(e->stream));
+  return 0;
+}
+
+extern "C" int dpsnn_create(const dpsnn_params *p, const dpsnn_options *opts, dpsnn_engine **out) {
+  if (!p || !out) return dpsnn_fail(DPSNN_E_PARAM, "null argument");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return dpsnn_fail(DPSNN_E_CUDA, "no CUDA device available");
+  dpsnn_engine *e = new dpsnn_engine();
+  if (opts && opts->device >= 0 && opts->device < ndev) {
+    e->device = opts->device;
+  } else {
+    cudaGetDevice(&e->device);
+  }
+  if (cudaSetDevice(e->device) != cudaSuccess || cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete e;
+    return dpsnn_fail(DPSNN_E_CUDA, "cannot set up device %d", e->device);
+  }
+  for (int k = 0; k < 12; k++) cudaEventCreate(&e->ev[k]);
+  int rc = engine_build(e, p, opts);
+  if (rc) {
+    dpsnn_destroy(e);
+    return rc;
+  }
+  *out = e;
+  return 0;
+}
+
+extern "C" void dpsnn_destroy(dpsnn_engine *e) {
+  if (!e) return;
+  cudaSetDevice(e->device);
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  for (void *q : e->allocs) cudaFree(q);
+  for (int k = 0; k < 12; k++) cudaEventDestroy(e->ev[k]);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+}
+
+static int check_flags(dpsnn_engine *e) {
+  uint32_t f = 0;
+  CK(cudaMemcpyAsync(&f, e->d.flags, 4, cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  if (!f) return 0;
+  if (f & F_TIME_WINDOW) return dpsnn_fail(DPSNN_E_MODEL, "ERROR in neu dynamic: input currentTime in wrong ms");
+  if (f & F_NO_TARGET) return dpsnn_fail(DPSNN_E_MODEL, "ERROR neuSpikToAxSp: no forw host targ for a spiking neuron");
+  if (f & F_TOO_MANY_INPUTS)
+    return dpsnn_fail(DPSNN_E_CAPACITY, "more than %d synaptic inputs on one neuron in one step", MAX_INPUTS_PER_STEP);
+  if (f & F_OVERFLOW) return dpsnn_fail(DPSNN_E_CAPACITY, "event overflow list full");
+  if (f & F_BATH_DRAWS) return dpsnn_fail(DPSNN_E_CAPACITY, "bath draw buffer exhausted");
+  return dpsnn_fail(DPSNN_E_MODEL, "device error flags 0x%x", f);
+}
+
+static void timed_launch_begin(dpsnn_engine *e, int k) {
+  if (e->timing) cudaEventRecord(e->ev[2 * k], e->stream);
+}
+static void timed_launch_end(dpsnn_engine *e, int k) {
+  if (e->timing) {
+    cudaEventRecord(e->ev[2 * k + 1], e->stream);
+    cudaEventSynchronize(e->ev[2 * k + 1]);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e->ev[2 * k], e->ev[2 * k + 1]);
+    e->ktime[k] += ms * 1e-3;
+    e->klaunch[k]++;
+  }
+}
+
+static int enqueue_step(dpsnn_engine *e) {
+  Dev &d = e->d;
+  timed_launch_begin(e, 0);
+  compact_kernel<<<e->grid_neuron, NEURON_BLOCK, 0, e->stream>>>(d);
+  timed_launch_end(e, 0);
+  if (e->hnet.stdp_on) {
+    timed_launch_begin(e, 4);
+    causal_stdp_kernel<<<e->grid_deliver, 256, 0, e->stream>>>(d);
+    timed_launch_end(e, 4);
+  }
+  timed_launch_begin(e, 1);
+  deliver_kernel<<<e->grid_deliver, 256, 0, e->stream>>>(d);
+  timed_launch_end(e, 1);
+  timed_launch_begin(e, 2);
+  bath_kernel<<<e->hnet.P, BATH_THREADS, 0, e->stream>>>(d);
+  timed_launch_end(e, 2);
+  timed_launch_begin(e, 3);
+  neuron_kernel<<<e->grid_neuron, NEURON_BLOCK, 0, e->stream>>>(d);
+  heavy_kernel<<<32, 64, 0, e->stream>>>(d);
+  timed_launch_end(e, 3);
+  if (e->hnet.stdp_on) {
+    timed_launch_begin(e, 4);
+    ltp_kernel<<<e->grid_deliver, 256, 0, e->stream>>>(d);
+    timed_launch_end(e, 4);
+  }
+  end_step_kernel<<<1, 1, 0, e->stream>>>(d);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return dpsnn_fail(DPSNN_E_CUDA, "kernel launch: %s", cudaGetErrorString(err));
+  e->t_host++;
+  return 0;
+}
+
+extern "C" int dpsnn_step(dpsnn_engine *e, uint32_t nsteps) {
+  if (!e) return dpsnn_fail(DPSNN_E_PARAM, "null engine");
+  cudaSetDevice(e->device);
+  for (uint32_t k = 0; k < nsteps; k++) {
+    int rc = enqueue_step(e);
+    if (rc) return rc;
+  }
+  return 0;
+}
+
+extern "C" int dpsnn_sync(dpsnn_engine *e) {
+  if (!e) return dpsnn_fail(DPSNN_E_PARAM, "null engine");
+  cudaSetDevice(e->device);
+  CK(cudaStreamSynchronize(e->stream));
+  return check_flags(e);
+}
+
+extern "C" uint32_t dpsnn_glob_n(const dpsnn_engine *e) { return e ? e->hnet.N : 0; }
+extern "C" uint32_t dpsnn_time_ms(const dpsnn_engine *e) { return e ? e->t_host : 0; }
+extern "C" uint64_t dpsnn_synapse_count(const dpsnn_engine *e) { return e ? e->S : 0; }
+extern "C" uint64_t dpsnn_events_delivered(const dpsnn_engine *e) {
+  if (!e) return 0;
+  unsigned long long v = 0;
+  cudaSetDevice(e->device);
+  cudaMemcpyAsync(&v, e->d.events, 8, cudaMemcpyDeviceToHost, e->stream);
+  cudaStreamSynchronize(e->stream);
+  return v;
+}
+
+extern "C" int dpsnn_spikes(dpsnn_engine *e, uint32_t t_ms, uint32_t *ids, double *te, uint32_t cap,
+                            uint32_t *count) {
+  if (!e || !count) return dpsnn_fail(DPSNN_E_PARAM, "null argument");
+  int rc = dpsnn_sync(e);
+  if (rc) return rc;
+  if (t_ms >= e->t_host || t_ms + RING_SLOTS <= e->t_host)
+    return dpsnn_fail(DPSNN_E_STATE, "step %u is not among the last %d completed steps", t_ms, RING_SLOTS);
+  uint32_t slot = t_ms % RING_SLOTS, cnt = 0;
+  CK(cudaMemcpy(&cnt, e->d.ring_cnt + slot, 4, cudaMemcpyDeviceToHost));
+  *count = cnt;
+  uint32_t k = std::min(cnt, cap);
+  if (k && ids) CK(cudaMemcpy(ids, e->d.ring_ids + (size_t)slot * e->hnet.N, 4ull * k, cudaMemcpyDeviceToHost));
+  if (k && te) CK(cudaMemcpy(te, e->d.ring_te + (size_t)slot * e->hnet.N, 8ull * k, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+extern "C" int dpsnn_state(dpsnn_engine *e, double *v, double *c, double *tr, double *te, double *nb) {
+  if (!e) return dpsnn_fail(DPSNN_E_PARAM, "null engine");
+  int rc = dpsnn_sync(e);
+  if (rc) return rc;
+  size_t B = 8ull * e->hnet.N;
+  if (v) CK(cudaMemcpy(v, e->d.v, B, cudaMemcpyDeviceToHost));
+  if (c) CK(cudaMemcpy(c, e->d.c, B, cudaMemcpyDeviceToHost));
+  if (tr) CK(cudaMemcpy(tr, e->d.tr, B, cudaMemcpyDeviceToHost));
+  if (te) CK(cudaMemcpy(te, e->d.te, B, cudaMemcpyDeviceToHost));
+  if (nb) CK(cudaMemcpy(nb, e->d.nb, B, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+extern "C" int dpsnn_bath_params(dpsnn_engine *e, double *inv_nu_ext, uint32_t *max_ext) {
+  if (!e) return dpsnn_fail(DPSNN_E_PARAM, "null engine");
+  int rc = dpsnn_sync(e);
+  if (rc) return rc;
+  if (inv_nu_ext) CK(cudaMemcpy(inv_nu_ext, e->d.inv_nu, 8ull * e->hnet.N, cudaMemcpyDeviceToHost));
+  if (max_ext) CK(cudaMemcpy(max_ext, e->d.max_ext, 4ull * e->hnet.N, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+// Host-side view of the connectome for the reference-order backward list.
+struct HostCsr {
+  std::vector<uint64_t> row;
+  std::vector<uint16_t> so;
+  std::vector<uint32_t> post;
+  std::vector<int16_t> w;
+  std::vector<float> td;
+  std::vector<uint8_t> sub;
+};
+static int fetch_csr(dpsnn_engine *e, HostCsr &h, bool with_td) {
+  int rc = dpsnn_sync(e);
+  if (rc) return rc;
+  const uint32_t N = e->hnet.N, D = e->hnet.D;
+  h.row.resize(N + 1);
+  h.so.resize((size_t)N * (D + 1));
+  h.post.resize(e->S);
+  h.w.resize(e->S);
+  h.sub.resize(N);
+  CK(cudaMemcpy(h.row.data(), e->d.row_ptr, 8ull * (N + 1), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(h.so.data(), e->d.sub_off, 2ull * N * (D + 1), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(h.post.data(), e->d.post, 4ull * e->S, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(h.w.data(), e->d.w16, 2ull * e->S, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(h.sub.data(), e->d.sub, N, cudaMemcpyDeviceToHost));
+  if (with_td && e->d.tderiv) {
+    h.td.resize(e->S);
+    CK(cudaMemcpy(h.td.data(), e->d.tderiv, 4ull * e->S, cudaMemcpyDeviceToHost));
+  }
+  return 0;
+}
+
+extern "C" uint64_t dpsnn_rank_synapse_count(dpsnn_engine *e, uint32_t h) {
+  if (!e || h >= e->hnet.P) return 0;
+  HostCsr c;
+  if (fetch_csr(e, c, false)) return 0;
+  uint64_t n = 0;
+  for (uint64_t k = 0; k < e->S; k++) n += (c.post[k] / e->hnet.locN == h);
+  return n;
+}
+
+extern "C" int dpsnn_backward_synapses(dpsnn_engine *e, uint32_t h, uint32_t *pre, uint32_t *post, uint8_t *delay,
+                                       uint8_t *kind, int16_t *weight, float *tderiv) {
+  if (!e) return dpsnn_fail(DPSNN_E_PARAM, "null engine");
+  if (h >= e->hnet.P) return dpsnn_fail(DPSNN_E_PARAM, "rank %u out of range", h);
+  HostCsr c;
+  int rc = fetch_csr(e, c, tderiv != nullptr);
+  if (rc) return rc;
+  // reference order (inflateIntermToBackwardSynList): delay, then source
+  // rank / presynaptic index, then generation order
+  const uint32_t N = e->hnet.N, D = e->hnet.D, locN = e->hnet.locN;
+  uint64_t o = 0;
+  for (uint32_t dl = 0; dl < D; dl++)
+    for (uint32_t P = 0; P < N; P++) {
+      uint64_t b = c.row[P] + c.so[(size_t)P * (D + 1) + dl], en = c.row[P] + c.so[(size_t)P * (D + 1) + dl + 1];
+      for (uint64_t k = b; k < en; k++) {
+        if (c.post[k] / locN != h) continue;
+        if (pre) pre[o] = P;
+        if (post) post[o] = c.post[k];
+        if (delay) delay[o] = (uint8_t)dl;
+        if (kind) kind[o] = c.sub[P];
+        if (weight) weight[o] = c.w[k];
+        if (tderiv) tderiv[o] = c.td.empty() ? 0.0f : c.td[k];
+        o++;
+      }
+    }
+  return 0;
+}
+
+extern "C" int dpsnn_set_timing(dpsnn_engine *e, int enable) {
+  if (!e) return dpsnn_fail(DPSNN_E_PARAM, "null engine");
+  e->timing = enable;
+  return 0;
+}
+
+extern "C" int dpsnn_kernel_times(dpsnn_engine *e, double *seconds5, uint64_t *launches5) {
+  if (!e) return dpsnn_fail(DPSNN_E_PARAM, "null engine");
+  for (int k = 0; k < 5; k++) {
+    if (seconds5) seconds5[k] = e->ktime[k];
+    if (launches5) launches5[k] = e->klaunch[k];
+  }
+  return 0;
+}

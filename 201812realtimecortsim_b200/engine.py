@@ -1,0 +1,258 @@
+"""ctypes binding of the engine's C ABI (include/dpsnn_b200.h).
+
+The engine library ``libdpsnn_b200.so`` is built in-tree by ``build()``
+(csrc/Makefile).  There is no fallback: if the library or a GPU is missing,
+constructing an :class:`Engine` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdpsnn_b200.so")
+MAX_SUB = 27
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("cfx", C.c_uint32), ("cfy", C.c_uint32), ("nsub", C.c_uint32),
+        ("count", C.c_uint32 * MAX_SUB),
+        ("JExt", C.c_float * MAX_SUB), ("DJExt", C.c_float * MAX_SUB), ("NuExt", C.c_float * MAX_SUB),
+        ("Tau", C.c_float * MAX_SUB), ("Theta", C.c_float * MAX_SUB), ("H", C.c_float * MAX_SUB),
+        ("Tarp", C.c_float * MAX_SUB), ("AlphaC", C.c_float * MAX_SUB), ("TauC", C.c_float * MAX_SUB),
+        ("gC", C.c_float * MAX_SUB),
+        ("J", C.c_float * (MAX_SUB * MAX_SUB)), ("DJ", C.c_float * (MAX_SUB * MAX_SUB)),
+        ("DMin", C.c_float * (MAX_SUB * MAX_SUB)), ("DMax", C.c_float * (MAX_SUB * MAX_SUB)),
+        ("stencil_dim", C.c_uint32),
+        ("spec", C.POINTER(C.c_float)),
+        ("bath", C.POINTER(C.c_uint32)),
+        ("D", C.c_uint32), ("glob_h", C.c_uint32), ("global_seed", C.c_uint32),
+        ("total_sim_time_ms", C.c_uint32),
+        ("start_plasticity_ms", C.c_uint32), ("stop_plasticity_ms", C.c_uint32),
+        ("min_syn_weight_f", C.c_float),
+        ("stdp_antiCausalCoeff", C.c_float), ("stdp_multiplier", C.c_float), ("stdp_tau_ms", C.c_float),
+        ("stdp_causalMax", C.c_float), ("stdp_antiCausalMax", C.c_float), ("stdp_tauDecay_s", C.c_float),
+        ("stdp_drift", C.c_float),
+        ("moduloSec", C.c_uint32), ("ratesSampling", C.c_uint32),
+        ("startStatFiles_s", C.c_uint32), ("stopStatFiles_s", C.c_uint32),
+        ("startRatesPerPop_s", C.c_uint32), ("stopRatesPerPop_s", C.c_uint32),
+        ("spikes_writeDisable", C.c_uint32), ("statRatesPerPop_writeDisable", C.c_uint32),
+        ("howManyOutputFiles", C.c_uint32),
+    ]
+
+
+class Options(C.Structure):
+    _fields_ = [("events_per_neuron", C.c_uint32), ("overflow_events", C.c_uint32), ("device", C.c_int)]
+
+
+EXPORTS = [
+    "dpsnn_params_from_env", "dpsnn_create", "dpsnn_destroy", "dpsnn_step", "dpsnn_sync",
+    "dpsnn_glob_n", "dpsnn_time_ms", "dpsnn_synapse_count", "dpsnn_events_delivered",
+    "dpsnn_spikes", "dpsnn_rank_synapse_count", "dpsnn_backward_synapses", "dpsnn_state",
+    "dpsnn_bath_params", "dpsnn_set_timing", "dpsnn_kernel_times", "dpsnn_last_error",
+]
+
+_LIB = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load the engine library (raises OSError when it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise OSError(f"{path} is missing: run __graft_entry__.build() first")
+    lib = C.CDLL(path)
+    P = C.c_void_p
+    lib.dpsnn_params_from_env.argtypes = [C.c_char_p, C.POINTER(Params)]
+    lib.dpsnn_create.argtypes = [C.POINTER(Params), C.POINTER(Options), C.POINTER(P)]
+    lib.dpsnn_destroy.argtypes = [P]
+    lib.dpsnn_destroy.restype = None
+    lib.dpsnn_step.argtypes = [P, C.c_uint32]
+    lib.dpsnn_sync.argtypes = [P]
+    lib.dpsnn_glob_n.argtypes = [P]
+    lib.dpsnn_glob_n.restype = C.c_uint32
+    lib.dpsnn_time_ms.argtypes = [P]
+    lib.dpsnn_time_ms.restype = C.c_uint32
+    lib.dpsnn_synapse_count.argtypes = [P]
+    lib.dpsnn_synapse_count.restype = C.c_uint64
+    lib.dpsnn_events_delivered.argtypes = [P]
+    lib.dpsnn_events_delivered.restype = C.c_uint64
+    lib.dpsnn_spikes.argtypes = [P, C.c_uint32, P, P, C.c_uint32, C.POINTER(C.c_uint32)]
+    lib.dpsnn_rank_synapse_count.argtypes = [P, C.c_uint32]
+    lib.dpsnn_rank_synapse_count.restype = C.c_uint64
+    lib.dpsnn_backward_synapses.argtypes = [P, C.c_uint32] + [P] * 6
+    lib.dpsnn_state.argtypes = [P] * 6
+    lib.dpsnn_bath_params.argtypes = [P, P, P]
+    lib.dpsnn_set_timing.argtypes = [P, C.c_int]
+    lib.dpsnn_kernel_times.argtypes = [P, P, P]
+    lib.dpsnn_last_error.restype = C.c_char_p
+    _LIB = lib
+    return lib
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class ParamsHolder:
+    """A Params struct together with the arrays its pointers refer to."""
+
+    def __init__(self, p: Params, spec: np.ndarray, bath: np.ndarray):
+        self.p, self.spec, self.bath = p, spec, bath
+
+
+def params_from_netconfig(cfg) -> ParamsHolder:
+    """Fill the engine's parameter struct from a ``netconfig.NetConfig``
+    (the values the reference would read from the files it writes)."""
+    p = Params()
+    nsub = len(cfg.subpops)
+    p.cfx, p.cfy, p.nsub = cfg.cfx, cfg.cfy, nsub
+    f32 = lambda v: float(np.float32(v))
+    for i, sp in enumerate(cfg.subpops):
+        p.count[i] = sp.count
+        for f in ("JExt", "DJExt", "NuExt", "Tau", "Theta", "H", "Tarp", "AlphaC", "TauC", "gC"):
+            getattr(p, f)[i] = f32(getattr(sp, f))
+    S = cfg.stencil_dim
+    spec = np.zeros((nsub, nsub, S, S), np.float32)
+    for (s, t), (J, DJ, dmin, dmax, probs) in cfg.conn.items():
+        p.J[s * nsub + t], p.DJ[s * nsub + t] = f32(J), f32(DJ)
+        p.DMin[s * nsub + t], p.DMax[s * nsub + t] = f32(dmin), f32(dmax)
+        for y in range(S):
+            for x in range(S):
+                spec[s, t, x, y] = probs[y * S + x]
+    bath = np.full((S, S), cfg.bath_cext, np.uint32)
+    spec = np.ascontiguousarray(spec)
+    p.stencil_dim = S
+    p.spec = spec.ctypes.data_as(C.POINTER(C.c_float))
+    p.bath = bath.ctypes.data_as(C.POINTER(C.c_uint32))
+    p.D, p.glob_h, p.global_seed = cfg.D, cfg.glob_h, cfg.seed
+    p.total_sim_time_ms = cfg.total_ms
+    p.start_plasticity_ms, p.stop_plasticity_ms = cfg.start_plasticity_ms, cfg.stop_plasticity_ms
+    p.min_syn_weight_f = f32(cfg.min_syn_weight_f)
+    if cfg.stdp is not None:
+        _, anti, mult, tau, cmax, amax, tdec, drift = cfg.stdp
+    else:
+        anti, mult, tau, cmax, amax, tdec, drift = -1.0, 0.001, 20.0, 0.1, 0.12, 1.0, 0.0
+    p.stdp_antiCausalCoeff, p.stdp_multiplier, p.stdp_tau_ms = f32(anti), f32(mult), f32(tau)
+    p.stdp_causalMax, p.stdp_antiCausalMax = f32(cmax), f32(amax)
+    p.stdp_tauDecay_s, p.stdp_drift = f32(tdec), f32(drift)
+    p.moduloSec, p.ratesSampling = 1, 5
+    p.startStatFiles_s, p.stopStatFiles_s = 0, 100000
+    p.startRatesPerPop_s, p.stopRatesPerPop_s = 0, 100000
+    p.howManyOutputFiles = 1
+    return ParamsHolder(p, spec, bath)
+
+
+class EngineError(RuntimeError):
+    pass
+
+
+class Engine:
+    """One network on one GPU."""
+
+    def __init__(self, params, events_per_neuron: int = 0, overflow_events: int = 0, device: int = -1):
+        self._L = load_library()
+        holder = params if isinstance(params, ParamsHolder) else params_from_netconfig(params)
+        self._holder = holder
+        opts = Options(events_per_neuron, overflow_events, device)
+        h = C.c_void_p()
+        rc = self._L.dpsnn_create(C.byref(holder.p), C.byref(opts), C.byref(h))
+        if rc != 0:
+            raise EngineError(f"dpsnn_create failed ({rc}): {self._L.dpsnn_last_error().decode()}")
+        self._h = h
+        self.glob_n = self._L.dpsnn_glob_n(h)
+        self.glob_h = holder.p.glob_h
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise EngineError(f"{what} failed ({rc}): {self._L.dpsnn_last_error().decode()}")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.dpsnn_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n: int = 1):
+        self._check(self._L.dpsnn_step(self._h, n), "dpsnn_step")
+
+    def sync(self):
+        self._check(self._L.dpsnn_sync(self._h), "dpsnn_sync")
+
+    @property
+    def time_ms(self) -> int:
+        return self._L.dpsnn_time_ms(self._h)
+
+    @property
+    def synapse_count(self) -> int:
+        return self._L.dpsnn_synapse_count(self._h)
+
+    def events_delivered(self) -> int:
+        return self._L.dpsnn_events_delivered(self._h)
+
+    def spikes(self, t_ms: int):
+        cnt = C.c_uint32()
+        self._check(self._L.dpsnn_spikes(self._h, t_ms, None, None, 0, C.byref(cnt)), "dpsnn_spikes")
+        n = cnt.value
+        ids = np.empty(n, np.uint32)
+        te = np.empty(n, np.float64)
+        if n:
+            self._check(self._L.dpsnn_spikes(self._h, t_ms, _ptr(ids), _ptr(te), n, C.byref(cnt)), "dpsnn_spikes")
+        return ids, te
+
+    def backward_synapses(self, rank: int = 0, with_tderiv: bool = False):
+        n = self._L.dpsnn_rank_synapse_count(self._h, rank)
+        pre = np.empty(n, np.uint32)
+        post = np.empty(n, np.uint32)
+        d = np.empty(n, np.uint8)
+        k = np.empty(n, np.uint8)
+        w = np.empty(n, np.int16)
+        td = np.empty(n, np.float32) if with_tderiv else None
+        self._check(self._L.dpsnn_backward_synapses(self._h, rank, _ptr(pre), _ptr(post), _ptr(d), _ptr(k),
+                                                     _ptr(w), _ptr(td)), "dpsnn_backward_synapses")
+        return (pre, post, d, k, w, td) if with_tderiv else (pre, post, d, k, w)
+
+    def state(self):
+        arrs = [np.empty(self.glob_n, np.float64) for _ in range(5)]
+        self._check(self._L.dpsnn_state(self._h, *[_ptr(a) for a in arrs]), "dpsnn_state")
+        return dict(zip(("v", "c", "tr", "te", "nb"), arrs))
+
+    def bath_params(self):
+        inv = np.empty(self.glob_n, np.float64)
+        mx = np.empty(self.glob_n, np.uint32)
+        self._check(self._L.dpsnn_bath_params(self._h, _ptr(inv), _ptr(mx)), "dpsnn_bath_params")
+        return inv, mx
+
+    def set_timing(self, on: bool):
+        self._check(self._L.dpsnn_set_timing(self._h, 1 if on else 0), "dpsnn_set_timing")
+
+    def kernel_times(self):
+        sec = np.zeros(5, np.float64)
+        cnt = np.zeros(5, np.uint64)
+        self._check(self._L.dpsnn_kernel_times(self._h, _ptr(sec), _ptr(cnt)), "dpsnn_kernel_times")
+        return sec, cnt
+
+
+def params_from_env(workdir: str) -> ParamsHolder:
+    """Parse env_* + input files in ``workdir`` with the engine's C parser."""
+    lib = load_library()
+    p = Params()
+    rc = lib.dpsnn_params_from_env(workdir.encode(), C.byref(p))
+    if rc != 0:
+        raise EngineError(f"dpsnn_params_from_env failed ({rc}): {lib.dpsnn_last_error().decode()}")
+    nsub, S = p.nsub, p.stencil_dim
+    spec = np.ctypeslib.as_array(p.spec, shape=(nsub * nsub * S * S,)).copy()
+    bath = np.ctypeslib.as_array(p.bath, shape=(S * S,)).copy()
+    p.spec = spec.ctypes.data_as(C.POINTER(C.c_float))
+    p.bath = bath.ctypes.data_as(C.POINTER(C.c_uint32))
+    return ParamsHolder(p, spec, bath)

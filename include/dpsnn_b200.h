@@ -1,0 +1,147 @@
+/*
+ * dpsnn_b200.h -- C ABI of the B200 engine for DPSNN's per-timestep loop.
+ *
+ * One engine simulates one DPSNN network (all env_globH ranks of it) on one
+ * GPU.  Plain C types only; every call returns 0 on success or a negative
+ * DPSNN_E_* code, with a message available from dpsnn_last_error().
+ *
+ * Correspondence with the reference interface each call replaces:
+ *   dpsnn_params_from_env  <- getParameters()             DPSNN_getParameters.c:23-831
+ *                             + describeConnectome() file parsing
+ *                                                         DPSNN_LIFCAconnectome.cpp:16-487
+ *                             + readPlasticityParametersFile()
+ *                                                         DPSNN_getParameters.c:900-1053
+ *   dpsnn_create           <- localNetClass::init()       DPSNN_localNet_init.c:43-307
+ *                             (synapse generation, connectome sort, neuron init,
+ *                              RNG seeding), one call for all ranks
+ *   dpsnn_step             <- localNetClass::completeTimeStep_ms()
+ *                                                         DPSNN_localNet_sim.c:22-307
+ *                             (+ stopWatch advance, localNetProcess.c:120-137)
+ *   dpsnn_spikes           <- the spike list handed to statSpikesClass::write
+ *                                                         DPSNN_localNet_sim.c:222-226
+ *   dpsnn_backward_synapses<- backwardSynList of rank h   DPSNN_localNet_init.c:591-617
+ *   dpsnn_destroy          <- process exit (the reference never frees)
+ * The DAL process trio localNetProcess_init/fire/finish and getParameters
+ * themselves, with C++ linkage as in the reference, are exported by
+ * libdpsnn_localnet.so (dpsnn_localnet.h).
+ */
+#ifndef DPSNN_B200_H
+#define DPSNN_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DPSNN_MAX_SUBPOP 27
+
+enum {
+  DPSNN_OK = 0,
+  DPSNN_E_PARAM = -1,      /* invalid or missing parameter / input file */
+  DPSNN_E_CUDA = -2,       /* CUDA runtime error */
+  DPSNN_E_NOMEM = -3,      /* device or host allocation failed */
+  DPSNN_E_CAPACITY = -4,   /* a fixed capacity was exceeded */
+  DPSNN_E_MODEL = -5,      /* a condition on which the reference exits */
+  DPSNN_E_STATE = -6       /* call not valid in the engine's current state */
+};
+
+/* Everything the reference reads from env_* variables and its four input
+ * files, already parsed (floats as atof() -> float gives them). */
+typedef struct {
+  /* grid and sub-populations (column.txt, env_CFX/env_CFY) */
+  uint32_t cfx, cfy, nsub;
+  uint32_t count[DPSNN_MAX_SUBPOP];
+  float JExt[DPSNN_MAX_SUBPOP], DJExt[DPSNN_MAX_SUBPOP], NuExt[DPSNN_MAX_SUBPOP];
+  float Tau[DPSNN_MAX_SUBPOP], Theta[DPSNN_MAX_SUBPOP], H[DPSNN_MAX_SUBPOP];
+  float Tarp[DPSNN_MAX_SUBPOP], AlphaC[DPSNN_MAX_SUBPOP], TauC[DPSNN_MAX_SUBPOP];
+  float gC[DPSNN_MAX_SUBPOP];
+  /* connectivity.txt, [src*nsub + tgt] */
+  float J[DPSNN_MAX_SUBPOP * DPSNN_MAX_SUBPOP];
+  float DJ[DPSNN_MAX_SUBPOP * DPSNN_MAX_SUBPOP];
+  float DMin[DPSNN_MAX_SUBPOP * DPSNN_MAX_SUBPOP];
+  float DMax[DPSNN_MAX_SUBPOP * DPSNN_MAX_SUBPOP];
+  uint32_t stencil_dim;           /* env_stencilDim (explicit stencil) */
+  /* spec[((src*nsub + tgt)*stencil_dim + x)*stencil_dim + y] */
+  const float *spec;
+  /* bathEfficacy.txt, bath[x*stencil_dim + y] */
+  const uint32_t *bath;
+  /* env_* */
+  uint32_t D;                     /* env_D */
+  uint32_t glob_h;                /* env_globH: ranks whose RNG streams are emulated */
+  uint32_t global_seed;           /* env_globalSeed */
+  uint32_t total_sim_time_ms;     /* env_totalSimTime_ms */
+  uint32_t start_plasticity_ms, stop_plasticity_ms;
+  float min_syn_weight_f;         /* env_minSynWeight_f */
+  /* plasticity.txt (Song STDP) */
+  float stdp_antiCausalCoeff, stdp_multiplier, stdp_tau_ms;
+  float stdp_causalMax, stdp_antiCausalMax, stdp_tauDecay_s, stdp_drift;
+  /* output controls (env_*) used by the stat writers */
+  uint32_t moduloSec, ratesSampling, startStatFiles_s, stopStatFiles_s;
+  uint32_t startRatesPerPop_s, stopRatesPerPop_s;
+  uint32_t spikes_writeDisable, statRatesPerPop_writeDisable, howManyOutputFiles;
+} dpsnn_params;
+
+/* Engine capacities (0 = default). */
+typedef struct {
+  uint32_t events_per_neuron;     /* synaptic events per neuron per step kept
+                                     in the fast path (default 64) */
+  uint32_t overflow_events;       /* events beyond that, per step (default 1<<22) */
+  int device;                     /* CUDA device ordinal (default current) */
+} dpsnn_options;
+
+typedef struct dpsnn_engine dpsnn_engine;
+
+/* Fill *p from the env_* variables and the input files in `workdir`
+ * (NULL = current directory).  Arrays spec/bath point into storage owned by
+ * the library until the next call of this function in the same thread. */
+int dpsnn_params_from_env(const char *workdir, dpsnn_params *p);
+
+/* Build the network on the GPU: synapse generation, connectome sort, neuron
+ * and RNG initialisation.  opts may be NULL. */
+int dpsnn_create(const dpsnn_params *p, const dpsnn_options *opts, dpsnn_engine **out);
+void dpsnn_destroy(dpsnn_engine *e);
+
+/* Run nsteps 1 ms steps (asynchronously; results are read by the calls below,
+ * which synchronise). */
+int dpsnn_step(dpsnn_engine *e, uint32_t nsteps);
+/* Block until all queued steps are done; reports a deferred device error. */
+int dpsnn_sync(dpsnn_engine *e);
+
+/* Sizes. */
+uint32_t dpsnn_glob_n(const dpsnn_engine *e);
+uint32_t dpsnn_time_ms(const dpsnn_engine *e);        /* steps completed */
+uint64_t dpsnn_synapse_count(const dpsnn_engine *e);
+/* Synaptic events delivered since creation. */
+uint64_t dpsnn_events_delivered(const dpsnn_engine *e);
+
+/* Spike list detected at step t_ms (one of the last 80 steps): ascending
+ * neuron index, with emission times.  *count receives the number of spikes;
+ * at most cap are written. */
+int dpsnn_spikes(dpsnn_engine *e, uint32_t t_ms, uint32_t *ids, double *te,
+                 uint32_t cap, uint32_t *count);
+
+/* Backward synapse list of rank h in the reference's memory order (sorted by
+ * delay, source rank, generation order), as dumped by synapticListReport.
+ * Arrays of dpsnn_rank_synapse_count() entries; any pointer may be NULL. */
+uint64_t dpsnn_rank_synapse_count(dpsnn_engine *e, uint32_t h);
+int dpsnn_backward_synapses(dpsnn_engine *e, uint32_t h, uint32_t *pre, uint32_t *post,
+                            uint8_t *delay, uint8_t *kind, int16_t *weight, float *tderiv);
+
+/* Neuron state, global neuron index order; any pointer may be NULL. */
+int dpsnn_state(dpsnn_engine *e, double *v, double *c, double *tr, double *te, double *nb);
+/* Per-neuron bath parameters (invNuExt, maxExternCurrentCount). */
+int dpsnn_bath_params(dpsnn_engine *e, double *inv_nu_ext, uint32_t *max_ext);
+
+/* Seconds of device time spent in each kernel family since creation
+ * (index: 0 compaction, 1 delivery, 2 bath, 3 neuron update, 4 plasticity);
+ * filled only when timing was enabled with dpsnn_set_timing(e, 1). */
+int dpsnn_set_timing(dpsnn_engine *e, int enable);
+int dpsnn_kernel_times(dpsnn_engine *e, double *seconds5, uint64_t *launches5);
+
+const char *dpsnn_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
