@@ -36,9 +36,9 @@
 #define MAX_INPUTS_PER_STEP 6000 // DSD__maxSimultaneousSpikesOnSameTarget
 #define MBIG 1000000000
 #define MSEED 161803398
-#define DRAW_RING (1u << 16)   // bath draws buffered per rank
 #define NEURON_BLOCK 256
-#define LOCAL_EVENTS 64        // per-thread event buffer of the neuron kernel
+#define LOCAL_EVENTS 32        // per-thread event buffer of the neuron kernel
+#define DEFAULT_EVENT_CAP 1024 // per-target event slots per step (capped by memory)
 
 // ------------------------------------------------------------------ errors
 static thread_local char g_err[1024];
@@ -98,7 +98,7 @@ struct NetConst {
   float causal_tab[128], anti_tab[128];
   float stdp_drift, stdp_tauDecay;
   uint32_t ev_cap, ovf_cap;
-  uint32_t bath_need;  // draws kept ahead of the bath consumer
+  uint32_t bath_need;  // largest maxExternCurrentCount
 };
 
 // ------------------------------------------------------------------ ran3
@@ -380,22 +380,19 @@ struct Dev {
   uint2 *ev;
   uint32_t *ovf_cnt;
   uint4 *ovf;
-  uint32_t *heavy_list, *heavy_cnt;
-  uint2 *heavy_scratch;     // {key, w} gathered for heavy neurons
-  double *heavy_tau;
-  uint32_t *heavy_scratch_used;
-  uint64_t heavy_scratch_cap;
+  uint32_t *heavy_list, *heavy_cnt;   // [2N]: neuron, event count
   // bath
   uint32_t *bath_hist;      // [P][64] ran3 history ring
   uint64_t *bath_produced, *bath_pos;  // [P]
-  uint8_t *draw_idx;        // [P][DRAW_RING]
-  float *draw_lapse;        // [P][DRAW_RING]
+  uint8_t *draw_idx;        // [P][BATH_RING] converted draws kept between steps
+  float *draw_lapse;        // [P][BATH_RING]
   uint64_t *bath_rank_base; // [P+1]
   uint32_t *bath_off;       // [N]
   uint16_t *bath_cnt;       // [N]
   double *bath_time;
   uint8_t *bath_lut;
   logf_fixup_t fix;
+  const uint32_t *fix_bitmap; // one bit per float in [0x30000000, 0x3F800000]: key has a fix-up
   // control
   uint32_t *t;              // current step
   uint32_t *flags;
@@ -532,122 +529,285 @@ __global__ void deliver_kernel(Dev d) {
 
 // Step 3: the Poisson bath (regularDynamicTimeStep, DPSNN_neuron_sim.c:604-640,
 // getPoissonLapse :844-865).  Each rank owns one serial ran3 stream that its
-// neurons consume in index order.  One block per rank: warp 0 extends the
-// lagged Fibonacci sequence 24 values per round (x[n] = x[n-55] - x[n-24]),
-// all warps turn new draws into the LUT index (uint32)(u*256) and the lapse
-// factor -logf((float)(1-u)), and thread 0 walks the neurons.
+// neurons consume in index order: a neuron whose next bath time is before
+// t+1 takes one pair of draws (LUT index, lapse) per event.  One block per
+// rank runs a shared-memory pipeline:
+//   warp 1     extends the lagged Fibonacci sequence 24 values per round
+//              (x[n] = x[n-55] - x[n-24] mod 1e9) into a ring of raw draws;
+//   warps 2..7 convert each round into the LUT index (uint32)(u*256) and the
+//              lapse factor -logf((float)(1-u));
+//   warp 0     walks the neurons: the serial chain only counts each neuron's
+//              events (all lanes in step, parameters passed by shuffles),
+//              then the 32 lanes write a 32-neuron chunk's events in
+//              parallel, each replaying its neuron from the chain's start.
+// Ring slots are published per 24-draw round with a flag; every wait is
+// bounded and raises F_BATH_DRAWS when its limit is reached.
 #define BATH_THREADS 256
-#define BATH_CHUNK 1536  // draws generated per refill (multiple of 24)
+#define BATH_RING 8192         // draws resident in shared memory
+#define BATH_ROUNDS 512        // round flags tracked (BATH_ROUNDS*24 > BATH_RING)
+#define BATH_MAX_EXT 2048      // largest maxExternCurrentCount supported
+#define BATH_SPIN_LIMIT (1u << 26)
 
-__device__ static inline float lapse_factor(logf_fixup_t fx, uint32_t mj) {
-  double u = mj * (1.0 / (double)MBIG);
+struct BathSmem {
+  float lap[BATH_RING];
+  uint32_t raw[BATH_RING];
+  uint8_t idx[BATH_RING];
+  uint32_t flag[BATH_ROUNDS];       // round r converted <=> flag[r % BATH_ROUNDS] == r + 1
+  uint32_t hist[64];
+  unsigned long long pos;           // consumer position (draws)
+  unsigned long long raw_end;       // draws generated
+  unsigned long long conv_base;     // first draw of round 0 of this launch
+  uint32_t next_round;              // next round a converter claims
+  uint32_t done, err;
+};
+
+// logf of the host C library on (0,1]: a one-bit-per-float filter, then a
+// binary search of the fix-up keys.
+__device__ static inline float logf_ref_dev(const logf_fixup_t &fx, const uint32_t *__restrict__ bitmap, float x) {
+  const float f = logf_cr_from(x, log((double)x));
+  union { float f; uint32_t u; } b;
+  b.f = x;
+  const uint32_t key = b.u;
+  if (key < 0x30000000u || key > 0x3F800000u) return f;
+  const uint32_t bit = key - 0x30000000u;
+  if (!((__ldg(&bitmap[bit >> 5]) >> (bit & 31)) & 1u)) return f;
+  uint32_t lo = 0, hi = fx.n;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(&fx.keys[mid]) < key) lo = mid + 1; else hi = mid;
+  }
+  return (lo < fx.n && __ldg(&fx.keys[lo]) == key) ? __ldg(&fx.vals[lo]) : f;
+}
+
+__device__ static inline void bath_convert(const Dev &d, BathSmem &s, unsigned long long n) {
+  const uint32_t k = (uint32_t)n & (BATH_RING - 1);
+  const uint32_t mj = s.raw[k];
+  const double u = mj * (1.0 / (double)MBIG);
+  s.idx[k] = (uint8_t)(uint32_t)(u * 256);
   double temp = (double)1.0 - u;
   if (temp < 0) temp = 0;
-  float x = (float)temp;
-  float lf = logf_fixup_lookup(fx, x, logf_cr_from(x, log((double)x)));
-  return -lf;
+  s.lap[k] = -logf_ref_dev(d.fix, d.fix_bitmap, (float)temp);
 }
 
 __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
+  extern __shared__ __align__(16) unsigned char bath_smem_raw[];
+  BathSmem &s = *reinterpret_cast<BathSmem *>(bath_smem_raw);
+  volatile BathSmem &vs = s;
   const NetConst *net = d.net;
-  const uint32_t h = blockIdx.x, t = *d.t;
-  const uint32_t tid = threadIdx.x;
-  __shared__ uint32_t s_hist[64];
-  __shared__ unsigned long long s_produced, s_pos;
-  __shared__ uint32_t s_next_i, s_done, s_out;
-  uint8_t *didx = d.draw_idx + (size_t)h * DRAW_RING;
-  float *dlap = d.draw_lapse + (size_t)h * DRAW_RING;
-  if (tid < 64) s_hist[tid] = d.bath_hist[h * 64 + tid];
+  const uint32_t h = blockIdx.x, t = *d.t, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // restore: generator history, consumer position, draws converted last launch
+  const unsigned long long p0 = d.bath_pos[h], q0 = d.bath_produced[h];
+  if (tid < 64) s.hist[tid] = d.bath_hist[h * 64 + tid];
+  for (unsigned long long n = p0 + tid; n < q0; n += blockDim.x) {
+    const uint32_t k = (uint32_t)n & (BATH_RING - 1);
+    s.lap[k] = d.draw_lapse[(size_t)h * BATH_RING + k];
+    s.idx[k] = d.draw_idx[(size_t)h * BATH_RING + k];
+  }
+  for (uint32_t r = tid; r < BATH_ROUNDS; r += blockDim.x) s.flag[r] = 0;
   if (tid == 0) {
-    s_produced = d.bath_produced[h];
-    s_pos = d.bath_pos[h];
-    s_next_i = 0;
-    s_done = 0;
-    s_out = 0;
+    s.pos = p0;
+    s.raw_end = q0;
+    s.conv_base = q0;
+    s.next_round = 0;
+    s.done = 0;
+    s.err = 0;
   }
   __syncthreads();
-  const double T0 = (double)t, T1 = (double)(T0 + 1.0);
+  const double T1 = (double)((double)t + 1.0);
   const uint32_t locN = net->locN, i0 = h * locN;
   const uint64_t ev_base = d.bath_rank_base[h];
-  while (true) {
-    // refill the draw ring ahead of the consumer
-    while ((long long)(s_produced - s_pos) < (long long)net->bath_need) {
-      unsigned long long n0 = s_produced;
-      if (tid < 32) {
-        for (int r = 0; r < BATH_CHUNK / 24; r++) {
-          uint32_t nn = (uint32_t)(n0 + (unsigned long long)r * 24 + tid);
-          int32_t x = 0;
-          if (tid < 24) {
-            x = (int32_t)s_hist[(nn - 55) & 63] - (int32_t)s_hist[(nn - 24) & 63];
-            if (x < 0) x += MBIG;
-          }
-          __syncwarp();
-          if (tid < 24) s_hist[nn & 63] = (uint32_t)x;
-          __syncwarp();
-          if (tid < 24) {
-            // raw draw kept in the lapse slot until all warps convert it
-            dlap[nn & (DRAW_RING - 1)] = __uint_as_float((uint32_t)x);
+
+  if (warp == 1) {
+    // ---- generator
+    uint32_t r = 0;
+    while (true) {
+      const unsigned long long n0 = s.conv_base + (unsigned long long)r * 24;
+      uint32_t spins = 0;
+      while (!vs.done && n0 + 24 > vs.pos + BATH_RING - 64) {
+        if (++spins > BATH_SPIN_LIMIT) { vs.err = 1; vs.done = 1; break; }
+      }
+      if (vs.done) break;
+      const uint32_t nn = (uint32_t)(n0 + lane);
+      int32_t x = 0;
+      if (lane < 24) {
+        x = (int32_t)s.hist[(nn - 55) & 63] - (int32_t)s.hist[(nn - 24) & 63];
+        if (x < 0) x += MBIG;
+      }
+      __syncwarp();
+      if (lane < 24) {
+        s.hist[nn & 63] = (uint32_t)x;
+        s.raw[nn & (BATH_RING - 1)] = (uint32_t)x;
+      }
+      __syncwarp();
+      __threadfence_block();
+      if (lane == 0) vs.raw_end = n0 + 24;
+      r++;
+    }
+  } else if (warp >= 2) {
+    // ---- converters
+    while (true) {
+      uint32_t r = 0;
+      if (lane == 0) r = atomicAdd(&s.next_round, 1u);
+      r = __shfl_sync(0xffffffffu, r, 0);
+      const unsigned long long n0 = s.conv_base + (unsigned long long)r * 24;
+      uint32_t spins = 0;
+      bool quit = false;
+      while (true) {
+        if (vs.raw_end >= n0 + 24) break;
+        if (vs.done) { quit = true; break; }
+        if (++spins > BATH_SPIN_LIMIT) { vs.err = 1; vs.done = 1; quit = true; break; }
+      }
+      if (quit) break;
+      __threadfence_block();
+      if (lane < 24) bath_convert(d, s, n0 + lane);
+      __syncwarp();
+      __threadfence_block();
+      if (lane == 0) vs.flag[r % BATH_ROUNDS] = r + 1;
+    }
+  } else {
+    // ---- consumer (warp 0)
+    unsigned long long pos = s.pos;
+    unsigned long long lim = s.raw_end;   // converted draws available (prefix)
+    uint32_t rr = 0;                      // next round to check
+    uint32_t out = 0;
+    bool fail = false;
+    double nx_nb = 0, nx_inv = 0;
+    uint32_t nx_mx = 0;
+    if (lane < min(32u, locN)) {
+      nx_nb = d.nb[i0 + lane];
+      nx_inv = d.inv_nu[i0 + lane];
+      nx_mx = d.max_ext[i0 + lane];
+    }
+    for (uint32_t c0 = 0; c0 < locN && !fail; c0 += 32) {
+      const uint32_t cn = min(32u, locN - c0);
+      const double my_nb = nx_nb, my_inv = nx_inv;
+      const uint32_t my_mx = nx_mx;
+      if (c0 + 32 < locN && lane < min(32u, locN - c0 - 32)) {   // prefetch the next chunk
+        nx_nb = d.nb[i0 + c0 + 32 + lane];
+        nx_inv = d.inv_nu[i0 + c0 + 32 + lane];
+        nx_mx = d.max_ext[i0 + c0 + 32 + lane];
+      }
+      unsigned long long my_start = 0;
+      uint32_t my_cnt = 0;
+      double nbv = __shfl_sync(0xffffffffu, my_nb, 0);
+      double inv = __shfl_sync(0xffffffffu, my_inv, 0);
+      uint32_t mx = __shfl_sync(0xffffffffu, my_mx, 0);
+      for (uint32_t j = 0; j < cn; j++) {
+        const uint32_t jn = (j + 1 < cn) ? j + 1 : j;
+        const double n_nb = __shfl_sync(0xffffffffu, my_nb, jn);
+        const double n_inv = __shfl_sync(0xffffffffu, my_inv, jn);
+        const uint32_t n_mx = __shfl_sync(0xffffffffu, my_mx, jn);
+        uint32_t spins = 0;
+        while (lim < pos + 2ull * mx + 4) {
+          if (vs.flag[rr % BATH_ROUNDS] == rr + 1) {
+            rr++;
+            lim = s.conv_base + (unsigned long long)rr * 24;
+            __threadfence_block();
+          } else if (++spins > BATH_SPIN_LIMIT) {
+            fail = true;
+            break;
           }
         }
-      }
-      __syncthreads();
-      for (uint32_t k = tid; k < BATH_CHUNK; k += blockDim.x) {
-        uint32_t nn = (uint32_t)(n0 + k) & (DRAW_RING - 1);
-        uint32_t mj = __float_as_uint(dlap[nn]);
-        didx[nn] = (uint8_t)(uint32_t)(mj * (1.0 / (double)MBIG) * 256);
-        dlap[nn] = lapse_factor(d.fix, mj);
-      }
-      __syncthreads();
-      if (tid == 0) s_produced = n0 + BATH_CHUNK;
-      __syncthreads();
-    }
-    if (tid == 0) {
-      unsigned long long pos = s_pos;
-      const unsigned long long lim = s_produced;
-      uint32_t i = s_next_i, out = s_out;
-      while (i < locN) {
-        uint32_t gi = i0 + i;
-        uint32_t mx = d.max_ext[gi];
-        if (lim - pos < 2ull * mx + 8) break;   // refill first
-        double inv = d.inv_nu[gi];
-        double nbv = d.nb[gi];
+        if (fail) break;
+        const unsigned long long start = pos;
         uint32_t c = 0;
-        d.bath_off[gi] = out;
-        if (inv > 0) {
-          if (nbv < T1) {
-            do {
-              d.bath_time[ev_base + out + c] = nbv;
-              d.bath_lut[ev_base + out + c] = didx[pos & (DRAW_RING - 1)];
-              c++;
-              nbv += (double)dlap[(pos + 1) & (DRAW_RING - 1)] * inv;
-              pos += 2;
-            } while ((nbv < T1) && (c < mx));
-            if (c >= mx && nbv < T1) {
-              do {
-                if (pos >= lim) { atomicOr(d.flags, F_BATH_DRAWS); break; }
-                nbv += (double)dlap[pos & (DRAW_RING - 1)] * inv;
-                pos += 1;
-              } while (nbv < T1);
-            }
+        if (inv > 0 && nbv < T1) {
+          float ln = s.lap[(pos + 1) & (BATH_RING - 1)];
+          do {
+            c++;
+            const double step = (double)ln * inv;
+            pos += 2;
+            ln = s.lap[(pos + 1) & (BATH_RING - 1)];
+            nbv += step;
+          } while ((nbv < T1) && (c < mx));
+          if (c >= mx && nbv < T1) {
+            do {   // single draws past the cap (rare)
+              while (lim <= pos) {
+                if (vs.flag[rr % BATH_ROUNDS] == rr + 1) {
+                  rr++;
+                  lim = s.conv_base + (unsigned long long)rr * 24;
+                  __threadfence_block();
+                } else if (++spins > BATH_SPIN_LIMIT) {
+                  fail = true;
+                  break;
+                }
+              }
+              if (fail) break;
+              nbv += (double)s.lap[pos & (BATH_RING - 1)] * inv;
+              pos += 1;
+            } while (nbv < T1);
           }
         }
-        d.nb[gi] = nbv;
-        d.bath_cnt[gi] = (uint16_t)c;
-        out += c;
-        i++;
+        if (fail) break;
+        if (lane == j) {
+          my_start = start;
+          my_cnt = c;
+        }
+        nbv = n_nb;
+        inv = n_inv;
+        mx = n_mx;
       }
-      s_next_i = i;
-      s_out = out;
-      s_pos = pos;
-      s_done = (i >= locN);
+      if (fail) break;
+      // parallel emission of the chunk's events
+      uint32_t incl = my_cnt;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += y;
+      }
+      const uint32_t my_off = out + incl - my_cnt;
+      out += __shfl_sync(0xffffffffu, incl, 31);
+      if (lane < cn) {
+        double v = my_nb;
+        unsigned long long p = my_start;
+        double *bt = d.bath_time + ev_base + my_off;
+        uint8_t *bl = d.bath_lut + ev_base + my_off;
+        for (uint32_t c = 0; c < my_cnt; c++) {
+          bt[c] = v;
+          bl[c] = s.idx[p & (BATH_RING - 1)];
+          v += (double)s.lap[(p + 1) & (BATH_RING - 1)] * my_inv;
+          p += 2;
+        }
+        if (my_cnt >= my_mx && my_cnt > 0 && v < T1) {
+          do {
+            v += (double)s.lap[p & (BATH_RING - 1)] * my_inv;
+            p += 1;
+          } while (v < T1);
+        }
+        d.nb[i0 + c0 + lane] = v;
+        d.bath_off[i0 + c0 + lane] = my_off;
+        d.bath_cnt[i0 + c0 + lane] = (uint16_t)my_cnt;
+      }
+      __syncwarp();
+      if (lane == 0) vs.pos = pos;   // ring slots before pos may now be reused
     }
-    __syncthreads();
-    if (s_done) break;
+    if (lane == 0) {
+      if (fail) vs.err = 1;
+      vs.pos = pos;
+      __threadfence_block();
+      vs.done = 1;
+    }
   }
-  if (tid < 64) d.bath_hist[h * 64 + tid] = s_hist[tid];
+  __syncthreads();
+  if (s.err) {
+    if (tid == 0) atomicOr(d.flags, F_BATH_DRAWS);
+    return;
+  }
+  // convert the generated rounds no converter reached, then save the state
+  const unsigned long long re = s.raw_end;
+  for (unsigned long long n = s.conv_base + tid; n < re; n += blockDim.x) {
+    const uint32_t r = (uint32_t)((n - s.conv_base) / 24);
+    if (s.flag[r % BATH_ROUNDS] != r + 1) bath_convert(d, s, n);
+  }
+  __syncthreads();
+  for (unsigned long long n = s.pos + tid; n < re; n += blockDim.x) {
+    const uint32_t k = (uint32_t)n & (BATH_RING - 1);
+    d.draw_lapse[(size_t)h * BATH_RING + k] = s.lap[k];
+    d.draw_idx[(size_t)h * BATH_RING + k] = s.idx[k];
+  }
+  if (tid < 64) d.bath_hist[h * 64 + tid] = s.hist[tid];
   if (tid == 0) {
-    d.bath_produced[h] = s_produced;
-    d.bath_pos[h] = s_pos;
+    d.bath_pos[h] = s.pos;
+    d.bath_produced[h] = re;
   }
 }
 
@@ -699,8 +859,8 @@ __device__ static inline double event_time(const Dev &d, uint32_t key, uint32_t 
 // Runs the merged event sequence of one neuron: synaptic events (sorted by
 // (time, key)) merged with the bath events (time-ordered), synaptic first on
 // equal times (mergeFunction, DPSNN_neuron_sim.c:391-421, called at :644-646).
-__device__ static inline void run_neuron(const Dev &d, uint32_t i, uint32_t t, const double *tau,
-                                         const float *val, uint32_t ns) {
+__device__ static inline int run_neuron(const Dev &d, uint32_t i, uint32_t t, const double *tau,
+                                        const float *val, uint32_t ns) {
   const NetConst *net = d.net;
   const uint32_t s = d.sub[i];
   NeuronRegs n;
@@ -735,20 +895,22 @@ __device__ static inline void run_neuron(const Dev &d, uint32_t i, uint32_t t, c
   d.tr[i] = n.tr;
   d.te[i] = n.te;
   if (n.fired) d.fired[i] = 1;
+  return n.fired;
 }
 
-// Step 4: neuron update, one thread per neuron (regularDynamicTimeStep,
-// DPSNN_neuron_sim.c:522-662).  Neurons with more events than the thread
-// buffer holds are queued for heavy_kernel.
+// Step 4: neuron update (regularDynamicTimeStep, DPSNN_neuron_sim.c:522-662).
+// Light neurons (at most LOCAL_EVENTS synaptic events this step): one thread
+// each, insertion sort by (arrival time, key) in registers/local memory.
+// Heavier neurons are queued for the heavy path below.
 __global__ void __launch_bounds__(NEURON_BLOCK) neuron_kernel(Dev d) {
   const NetConst *net = d.net;
   const uint32_t t = *d.t, N = net->N, D = net->D, cap = net->ev_cap;
   const uint32_t i = blockIdx.x * NEURON_BLOCK + threadIdx.x;
   int fired = 0;
   if (i < N) {
-    uint32_t cnt = d.ev_cnt[i];
+    const uint32_t cnt = d.ev_cnt[i];
     d.ev_cnt[i] = 0;
-    if (cnt > cap || cnt > LOCAL_EVENTS) {
+    if (cnt > LOCAL_EVENTS) {
       uint32_t k = atomicAdd(d.heavy_cnt, 1u);
       if (k < N) {
         d.heavy_list[k] = i;
@@ -760,9 +922,8 @@ __global__ void __launch_bounds__(NEURON_BLOCK) neuron_kernel(Dev d) {
       uint32_t key[LOCAL_EVENTS];
       const uint2 *ev = d.ev + (size_t)i * cap;
       for (uint32_t e = 0; e < cnt; e++) {
-        uint2 x = ev[e];
-        double tm = event_time(d, x.x, t, D, N);
-        // stable insertion by (time, key)
+        const uint2 x = ev[e];
+        const double tm = event_time(d, x.x, t, D, N);
         uint32_t p = e;
         while (p > 0 && (tau[p - 1] > tm || (tau[p - 1] == tm && key[p - 1] > x.x))) {
           tau[p] = tau[p - 1];
@@ -774,58 +935,211 @@ __global__ void __launch_bounds__(NEURON_BLOCK) neuron_kernel(Dev d) {
         val[p] = __uint_as_float(x.y);
         key[p] = x.x;
       }
-      run_neuron(d, i, t, tau, val, cnt);
-      fired = d.fired[i];
+      fired = run_neuron(d, i, t, tau, val, cnt);
     }
   }
-  uint32_t bc = __syncthreads_count(fired);
+  const uint32_t bc = __syncthreads_count(fired);
   if (threadIdx.x == 0) d.block_fired[blockIdx.x] = bc;
 }
 
-// Neurons with many events in one step: gather bucket + overflow events into
-// global scratch, sort by (time, key), run.  The last block also advances
-// the step counter.
-__global__ void heavy_kernel(Dev d) {
-  const NetConst *net = d.net;
-  const uint32_t t = *d.t, N = net->N, D = net->D, cap = net->ev_cap;
-  const uint32_t nh = min(*d.heavy_cnt, N);
-  const uint32_t novf = min(*d.ovf_cnt, net->ovf_cap);
-  for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < nh; h += gridDim.x * blockDim.x) {
-    uint32_t i = d.heavy_list[h], cnt = d.heavy_list[N + h];
-    if (cnt > MAX_INPUTS_PER_STEP) {
-      atomicOr(d.flags, F_TOO_MANY_INPUTS);
-      continue;
-    }
-    unsigned long long off = atomicAdd((unsigned long long *)d.heavy_scratch_used, (unsigned long long)cnt);
-    if (off + cnt > d.heavy_scratch_cap) {
-      atomicOr(d.flags, F_OVERFLOW);
-      continue;
-    }
-    uint2 *ks = d.heavy_scratch + off;
-    double *ts = d.heavy_tau + off;
-    uint32_t k = 0;
-    for (uint32_t e = 0; e < min(cnt, cap); e++) ks[k++] = d.ev[(size_t)i * cap + e];
-    for (uint32_t o = 0; o < novf && k < cnt; o++) {
-      uint4 x = d.ovf[o];
-      if (x.x == i) ks[k++] = make_uint2(x.y, x.z);
-    }
-    for (uint32_t e = 0; e < k; e++) {
-      uint2 x = ks[e];
-      double tm = event_time(d, x.x, t, D, N);
-      uint32_t p = e;
-      while (p > 0 && (ts[p - 1] > tm || (ts[p - 1] == tm && ks[p - 1].x > x.x))) {
-        ts[p] = ts[p - 1];
-        ks[p] = ks[p - 1];
-        p--;
+// Heavy neurons, more than LOCAL_EVENTS synaptic events in one step.
+// heavy_sort_kernel: one warp per neuron loads its bucket into shared memory,
+// computes the arrival times, bitonic-sorts by (time, key) and writes the
+// sorted events back into the bucket; heavy_run_kernel then runs the neurons
+// one thread each.  Neurons with more events than the bucket holds (the rest
+// sit in the overflow list) are sorted and run by huge_kernel, one block each.
+#define HEAVY_WARP_MAX 1024
+#define HEAVY_SORT_WARPS 4
+#define HEAVY_SORT_SMEM (HEAVY_SORT_WARPS * HEAVY_WARP_MAX * 16)
+#define HEAVY_MAX 8192
+#define HEAVY_THREADS 256
+#define HEAVY_SMEM (HEAVY_MAX * 16)
+
+__device__ static inline void bitonic_sort_shared(double *tau, uint32_t *key, float *val, uint32_t n2,
+                                                  uint32_t tid, uint32_t nthr, bool warp_only) {
+  for (uint32_t k = 2; k <= n2; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t a = tid; a < n2; a += nthr) {
+        const uint32_t b = a ^ j;
+        if (b > a) {
+          const bool up = (a & k) == 0;
+          const double ta = tau[a], tb = tau[b];
+          const uint32_t ka = key[a], kb = key[b];
+          const bool gt = (ta > tb) || (ta == tb && ka > kb);
+          if (gt == up) {
+            tau[a] = tb;
+            tau[b] = ta;
+            key[a] = kb;
+            key[b] = ka;
+            const float va = val[a];
+            val[a] = val[b];
+            val[b] = va;
+          }
+        }
       }
-      ts[p] = tm;
-      ks[p] = x;
+      if (warp_only) __syncwarp(); else __syncthreads();
     }
-    // run_neuron takes separate value array: reuse the key slots' y halves
-    float *vals = (float *)(d.heavy_tau + d.heavy_scratch_cap) + off;
-    for (uint32_t e = 0; e < k; e++) vals[e] = __uint_as_float(ks[e].y);
-    run_neuron(d, i, t, ts, vals, k);
-    if (d.fired[i]) atomicAdd(&d.block_fired[i / NEURON_BLOCK], 1u);
+  }
+}
+
+// Events per neuron handled by the warp path: at most the bucket size.
+__device__ static inline uint32_t warp_path_max(const NetConst *net) {
+  return min(net->ev_cap, (uint32_t)HEAVY_WARP_MAX);
+}
+
+__global__ void __launch_bounds__(HEAVY_SORT_WARPS * 32) heavy_sort_kernel(Dev d) {
+  extern __shared__ __align__(16) unsigned char hs_raw[];
+  const NetConst *net = d.net;
+  const uint32_t t = *d.t, N = net->N, D = net->D, cap = net->ev_cap, wmax = warp_path_max(net);
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double *tau_base = reinterpret_cast<double *>(hs_raw);
+  uint32_t *key_base = reinterpret_cast<uint32_t *>(tau_base + HEAVY_SORT_WARPS * HEAVY_WARP_MAX);
+  float *val_base = reinterpret_cast<float *>(key_base + HEAVY_SORT_WARPS * HEAVY_WARP_MAX);
+  double *tau = tau_base + (size_t)w * HEAVY_WARP_MAX;
+  uint32_t *key = key_base + (size_t)w * HEAVY_WARP_MAX;
+  float *val = val_base + (size_t)w * HEAVY_WARP_MAX;
+  const uint32_t nh = min(*d.heavy_cnt, N);
+  for (uint32_t hh = blockIdx.x * HEAVY_SORT_WARPS + w; hh < nh; hh += gridDim.x * HEAVY_SORT_WARPS) {
+    const uint32_t i = d.heavy_list[hh], n = d.heavy_list[N + hh];
+    if (n > wmax) continue;   // huge_kernel
+    uint2 *ev = d.ev + (size_t)i * cap;
+    uint32_t n2 = 1;
+    while (n2 < n) n2 <<= 1;
+    for (uint32_t e = lane; e < n2; e += 32) {
+      if (e < n) {
+        const uint2 x = ev[e];
+        key[e] = x.x;
+        val[e] = __uint_as_float(x.y);
+        tau[e] = event_time(d, x.x, t, D, N);
+      } else {
+        tau[e] = INFINITY;
+        key[e] = 0xFFFFFFFFu;
+      }
+    }
+    __syncwarp();
+    bitonic_sort_shared(tau, key, val, n2, lane, 32, true);
+    for (uint32_t e = lane; e < n; e += 32) ev[e] = make_uint2(key[e], __float_as_uint(val[e]));
+    __syncwarp();
+  }
+}
+
+// Runs a neuron whose events sit sorted in its bucket (arrival times are
+// recomputed from the keys); same merge and arithmetic as run_neuron.
+__global__ void heavy_run_kernel(Dev d) {
+  const NetConst *net = d.net;
+  const uint32_t t = *d.t, N = net->N, D = net->D, cap = net->ev_cap, wmax = warp_path_max(net);
+  const uint32_t nh = min(*d.heavy_cnt, N);
+  for (uint32_t hh = blockIdx.x * blockDim.x + threadIdx.x; hh < nh; hh += gridDim.x * blockDim.x) {
+    const uint32_t i = d.heavy_list[hh], ns = d.heavy_list[N + hh];
+    if (ns > wmax) continue;
+    const uint2 *ev = d.ev + (size_t)i * cap;
+    const uint32_t s = d.sub[i];
+    NeuronRegs n;
+    n.v = d.v[i];
+    n.c = d.c[i];
+    n.tr = d.tr[i];
+    n.te = d.te[i];
+    n.fired = 0;
+    const double T0 = (double)t;
+    const uint32_t bc = d.bath_cnt[i];
+    const uint64_t bbase = d.bath_rank_base[i / net->locN] + d.bath_off[i];
+    const double *lut = d.lut + (size_t)s * 256;
+    uint32_t a = 0, b = 0;
+    double bt = (b < bc) ? d.bath_time[bbase] : 0.0;
+    uint2 x = ev[0];
+    double at = event_time(d, x.x, t, D, N);
+    while (a < ns || b < bc) {
+      double ct, I;
+      if (a < ns && (b >= bc || at <= bt)) {
+        ct = at;
+        I = (double)__uint_as_float(x.y);
+        a++;
+        if (a < ns) {
+          x = ev[a];
+          at = event_time(d, x.x, t, D, N);
+        }
+      } else {
+        ct = bt;
+        I = lut[d.bath_lut[bbase + b]];
+        b++;
+        if (b < bc) bt = d.bath_time[bbase + b];
+      }
+      if (((ct - T0) >= 1.0) || ((ct - T0) < 0)) atomicOr(d.flags, F_TIME_WINDOW);
+      lifca(net, s, n, ct, I);
+    }
+    d.v[i] = n.v;
+    d.c[i] = n.c;
+    d.tr[i] = n.tr;
+    d.te[i] = n.te;
+    if (n.fired) {
+      d.fired[i] = 1;
+      atomicAdd(&d.block_fired[i / NEURON_BLOCK], 1u);
+    }
+  }
+}
+
+// Gather a neuron's events (bucket, then overflow list) into shared arrays.
+__device__ static inline uint32_t gather_events(const Dev &d, uint32_t i, uint32_t cnt, uint32_t *key, float *val,
+                                                uint32_t capacity, uint32_t tid, uint32_t nthr, uint32_t *counter) {
+  const NetConst *net = d.net;
+  const uint32_t cap = net->ev_cap, nb = min(cnt, cap);
+  for (uint32_t e = tid; e < nb; e += nthr) {
+    const uint2 x = d.ev[(size_t)i * cap + e];
+    key[e] = x.x;
+    val[e] = __uint_as_float(x.y);
+  }
+  if (tid == 0) *counter = nb;
+  __syncthreads();
+  if (cnt > cap) {
+    const uint32_t novf = min(*d.ovf_cnt, net->ovf_cap);
+    for (uint32_t o = tid; o < novf; o += nthr) {
+      const uint4 x = d.ovf[o];
+      if (x.x == i) {
+        uint32_t k = atomicAdd(counter, 1u);
+        if (k < capacity) {
+          key[k] = x.y;
+          val[k] = __uint_as_float(x.z);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  return min(*counter, capacity);
+}
+
+__global__ void __launch_bounds__(HEAVY_THREADS) huge_kernel(Dev d) {
+  extern __shared__ __align__(16) unsigned char heavy_smem_raw[];
+  double *s_tau = reinterpret_cast<double *>(heavy_smem_raw);
+  uint32_t *s_key = reinterpret_cast<uint32_t *>(s_tau + HEAVY_MAX);
+  float *s_val = reinterpret_cast<float *>(s_key + HEAVY_MAX);
+  __shared__ uint32_t s_n;
+  const NetConst *net = d.net;
+  const uint32_t t = *d.t, N = net->N, D = net->D, tid = threadIdx.x;
+  const uint32_t nh = min(*d.heavy_cnt, N);
+  for (uint32_t hh = blockIdx.x; hh < nh; hh += gridDim.x) {
+    const uint32_t i = d.heavy_list[hh], cnt = d.heavy_list[N + hh];
+    if (cnt <= warp_path_max(net)) continue;
+    if (cnt > MAX_INPUTS_PER_STEP) {
+      if (tid == 0) atomicOr(d.flags, F_TOO_MANY_INPUTS);
+      continue;
+    }
+    const uint32_t n = gather_events(d, i, cnt, s_key, s_val, HEAVY_MAX, tid, blockDim.x, &s_n);
+    uint32_t n2 = 1;
+    while (n2 < n) n2 <<= 1;
+    for (uint32_t e = tid; e < n2; e += blockDim.x) {
+      if (e < n) {
+        s_tau[e] = event_time(d, s_key[e], t, D, N);
+      } else {
+        s_tau[e] = INFINITY;
+        s_key[e] = 0xFFFFFFFFu;
+      }
+    }
+    __syncthreads();
+    bitonic_sort_shared(s_tau, s_key, s_val, n2, tid, blockDim.x, false);
+    if (tid == 0) {
+      if (run_neuron(d, i, t, s_tau, s_val, n)) atomicAdd(&d.block_fired[i / NEURON_BLOCK], 1u);
+    }
+    __syncthreads();
   }
 }
 
@@ -867,7 +1181,6 @@ __global__ void ltp_kernel(Dev d) {
 __global__ void end_step_kernel(Dev d) {
   *d.ovf_cnt = 0;
   *d.heavy_cnt = 0;
-  *d.heavy_scratch_used = 0;
   *d.t = *d.t + 1;
 }
 
@@ -944,7 +1257,7 @@ struct dpsnn_engine {
   uint64_t S = 0;
   uint32_t t_host = 0;   // steps enqueued
   std::vector<void *> allocs;
-  uint32_t grid_neuron = 0, grid_deliver = 0;
+  uint32_t grid_neuron = 0, grid_deliver = 0, grid_heavy = 0;
   int timing = 0;
   cudaEvent_t ev[12];
   double ktime[5] = {0, 0, 0, 0, 0};
@@ -1001,6 +1314,17 @@ static int load_logf_fixup(dpsnn_engine *e) {
   e->d.fix.vals = v;
   e->d.fix.bucket = b;
   e->d.fix.n = n;
+  {
+    const size_t words = ((size_t)(0x3F800000u - 0x30000000u) + 1 + 31) / 32;
+    std::vector<uint32_t> bm(words, 0u);
+    for (uint32_t key : e->fix_keys)
+      if (key >= 0x30000000u && key <= 0x3F800000u) bm[(key - 0x30000000u) >> 5] |= 1u << ((key - 0x30000000u) & 31);
+    uint32_t *dbm;
+    DALLOC(dbm, words);
+    CK(cudaMemcpyAsync(dbm, bm.data(), 4 * words, cudaMemcpyHostToDevice, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    e->d.fix_bitmap = dbm;
+  }
   return 0;
 }
 
@@ -1131,8 +1455,11 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
   for (int i = 1; i < 128; i++) n.anti_tab[i] = (1 - 1 / p->stdp_tau_ms) * n.anti_tab[i - 1];
   n.stdp_drift = p->stdp_drift;
   n.stdp_tauDecay = p->stdp_tauDecay_s;
-  n.ev_cap = (o && o->events_per_neuron) ? o->events_per_neuron : LOCAL_EVENTS;
-  if (n.ev_cap > LOCAL_EVENTS) n.ev_cap = LOCAL_EVENTS;
+  n.ev_cap = (o && o->events_per_neuron) ? o->events_per_neuron : DEFAULT_EVENT_CAP;
+  if (n.ev_cap > 4096) n.ev_cap = 4096;
+  if (!(o && o->events_per_neuron)) {   // default: at most 16 GiB of event slots
+    while (n.ev_cap > 64 && 8ull * n.ev_cap * n.N > (16ull << 30)) n.ev_cap >>= 1;
+  }
   n.ovf_cap = (o && o->overflow_events) ? o->overflow_events : (1u << 22);
 
   Dev &d = e->d;
@@ -1335,10 +1662,6 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
   DALLOC(d.ovf, n.ovf_cap);
   DALLOC(d.heavy_list, 2ull * N);
   DALLOC(d.heavy_cnt, 1);
-  d.heavy_scratch_cap = (uint64_t)n.ovf_cap + 64ull * MAX_INPUTS_PER_STEP;
-  DALLOC(d.heavy_scratch, d.heavy_scratch_cap);
-  DALLOC(d.heavy_tau, d.heavy_scratch_cap * 2);   // times, then float values
-  DALLOC(d.heavy_scratch_used, 2);
   DALLOC(d.t, 1);
   DALLOC(d.flags, 4);
   DALLOC(d.events, 1);
@@ -1357,9 +1680,11 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
     }
     uint32_t mx_max = 0;
     for (uint32_t i = 0; i < N; i++) mx_max = std::max(mx_max, mx[i]);
-    if (mx_max > 8192)
-      return dpsnn_fail(DPSNN_E_CAPACITY, "maxExternCurrentCount %u exceeds the bath buffer (8192)", mx_max);
-    n.bath_need = 2 * BATH_CHUNK + 2 * mx_max + 16;
+    // one 32-neuron chunk plus one neuron's look-ahead must fit in the draw ring
+    if (mx_max > BATH_MAX_EXT || 66ull * mx_max + 200 > BATH_RING)
+      return dpsnn_fail(DPSNN_E_CAPACITY, "maxExternCurrentCount %u exceeds what the bath ring holds (%d)", mx_max,
+                        (BATH_RING - 200) / 66);
+    n.bath_need = mx_max;
     CK(cudaMemcpyAsync(d.net, &n, sizeof n, cudaMemcpyHostToDevice, e->stream));
     DALLOC(d.bath_rank_base, P + 1);
     CK(cudaMemcpyAsync(d.bath_rank_base, base.data(), 8ull * (P + 1), cudaMemcpyHostToDevice, e->stream));
@@ -1405,8 +1730,8 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
     DALLOC(d.bath_hist, (size_t)P * 64);
     DALLOC(d.bath_produced, P);
     DALLOC(d.bath_pos, P);
-    DALLOC(d.draw_idx, (size_t)P * DRAW_RING);
-    DALLOC(d.draw_lapse, (size_t)P * DRAW_RING);
+    DALLOC(d.draw_idx, (size_t)P * BATH_RING);
+    DALLOC(d.draw_lapse, (size_t)P * BATH_RING);
     CK(cudaMemcpyAsync(d.bath_hist, hist.data(), 4ull * P * 64, cudaMemcpyHostToDevice, e->stream));
     CK(cudaMemcpyAsync(d.bath_produced, produced.data(), 8ull * P, cudaMemcpyHostToDevice, e->stream));
     CK(cudaMemcpyAsync(d.bath_pos, pos.data(), 8ull * P, cudaMemcpyHostToDevice, e->stream));
@@ -1418,6 +1743,10 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
   e->grid_deliver = (uint32_t)sms * 8;
+  e->grid_heavy = (uint32_t)sms * 4;
+  CK(cudaFuncSetAttribute(bath_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(BathSmem)));
+  CK(cudaFuncSetAttribute(huge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, HEAVY_SMEM));
+  CK(cudaFuncSetAttribute(heavy_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, HEAVY_SORT_SMEM));
   CK(cudaStreamSynchronize(e->stream));
   return 0;
 }
@@ -1500,11 +1829,13 @@ static int enqueue_step(dpsnn_engine *e) {
   deliver_kernel<<<e->grid_deliver, 256, 0, e->stream>>>(d);
   timed_launch_end(e, 1);
   timed_launch_begin(e, 2);
-  bath_kernel<<<e->hnet.P, BATH_THREADS, 0, e->stream>>>(d);
+  bath_kernel<<<e->hnet.P, BATH_THREADS, sizeof(BathSmem), e->stream>>>(d);
   timed_launch_end(e, 2);
   timed_launch_begin(e, 3);
   neuron_kernel<<<e->grid_neuron, NEURON_BLOCK, 0, e->stream>>>(d);
-  heavy_kernel<<<32, 64, 0, e->stream>>>(d);
+  heavy_sort_kernel<<<e->grid_heavy, HEAVY_SORT_WARPS * 32, HEAVY_SORT_SMEM, e->stream>>>(d);
+  heavy_run_kernel<<<e->grid_heavy, 128, 0, e->stream>>>(d);
+  huge_kernel<<<e->grid_heavy, HEAVY_THREADS, HEAVY_SMEM, e->stream>>>(d);
   timed_launch_end(e, 3);
   if (e->hnet.stdp_on) {
     timed_launch_begin(e, 4);
