@@ -1,0 +1,21 @@
+"""Networks pinned by the golden fixtures (see make_golden.py)."""
+import importlib
+
+nc = importlib.import_module("201812realtimecortsim_b200.netconfig")
+
+
+def small(cfx, cfy, ms=300, mu=0.6, **kw):
+    """Modules of 40+40 excitatory and 20 inhibitory neurons."""
+    return nc.cortical_grid(cfx, cfy, n_exc_a=40, n_exc_b=40, n_inh=20, p1=0.2, total_ms=ms, mu=mu, **kw)
+
+
+CASES = {
+    # one module of 100 neurons
+    "small_1x1": lambda: small(1, 1),
+    # 2x2 modules of 100 neurons, seed 7
+    "small_2x2": lambda: small(2, 2, seed=7),
+    # same grid with Song STDP from t=0 through two weight updates (x999 ms)
+    "small_2x2_stdp": lambda: small(2, 2, ms=2100, stdp=True, start_plasticity_ms=0),
+    # the 2x2 benchmark network: 5000 neurons, ~5.6 M synapses, 1 s
+    "c1_2x2": lambda: nc.cortical_grid(2, 2, total_ms=1000),
+}

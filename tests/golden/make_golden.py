@@ -1,0 +1,96 @@
+"""Generate the golden fixtures of tests/golden from the reference itself.
+
+Runs in the development container only (it needs the reference sources,
+compiled by ``make -C oracle ref kat``); the fixtures it writes are committed
+and are all the GPU box sees.  Each network is described by
+``201812realtimecortsim_b200.netconfig`` and run with the reference binaries
+built from the unmodified sources plus the bounds fix:
+
+* ``ref_kat.txt``        ran3 / NormDev / Gaussian LUT / roundr2i values from
+                          the reference's own randdev.o and erflib.o;
+* ``<case>.raster.gz``   full-precision raster (%.17g) of the reference;
+* ``<case>.spikes.gz``   the reference's own spikes file (%.7g);
+* ``manifest.json``      sha256 of the BACKWARD synapse dump and of the
+                          output files, spike counts, configuration.
+
+Usage: python tests/golden/make_golden.py
+"""
+import gzip
+import hashlib
+import importlib
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+from tests.golden.cases import CASES  # noqa: E402
+
+nc = importlib.import_module("201812realtimecortsim_b200.netconfig")
+REF_HP = os.path.join(ROOT, "oracle", "_ref", "dpsnn_ref_hp")
+REF = os.path.join(ROOT, "oracle", "_ref", "dpsnn_ref")
+KAT = os.path.join(ROOT, "oracle", "_ref", "ref_kat")
+
+
+def sha256(path):
+    h = hashlib.sha256()
+    with open(path, "rb") as f:
+        for chunk in iter(lambda: f.read(1 << 20), b""):
+            h.update(chunk)
+    return h.hexdigest()
+
+
+def run(binary, cfg, workdir):
+    env = dict(os.environ)
+    env.update(cfg.write(workdir))
+    r = subprocess.run([binary], cwd=workdir, env=env, capture_output=True, text=True)
+    if r.returncode != 0 or "ERROR" in r.stdout:
+        raise RuntimeError(r.stdout[-2000:] + r.stderr[-2000:])
+
+
+def main():
+    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", "kat"], check=True,
+                   capture_output=True)
+    with open(os.path.join(HERE, "ref_kat.txt"), "w") as f:
+        f.write(subprocess.run([KAT], check=True, capture_output=True, text=True).stdout)
+    manifest = {}
+    for name, make in CASES.items():
+        cfg = make()
+        entry = {"total_ms": cfg.total_ms, "glob_h": cfg.glob_h}
+        with tempfile.TemporaryDirectory() as td:
+            hp = os.path.join(td, "hp")
+            run(REF_HP, cfg, hp)
+            dump = [f for f in os.listdir(hp) if "SynapticList_BACKWARD" in f][0]
+            entry["backward_dump"] = dump
+            entry["backward_sha256"] = sha256(os.path.join(hp, dump))
+            lines = []
+            for sec in range((cfg.total_ms + 999) // 1000):
+                fn = os.path.join(hp, f"spikes-sec{sec}-C{cfg.n_modules}-H{cfg.glob_h}-h000.dat")
+                if os.path.exists(fn):
+                    with open(fn) as f:
+                        lines += f.readlines()
+            entry["spikes"] = len(lines)
+            with gzip.open(os.path.join(HERE, f"{name}.raster.gz"), "wt") as f:
+                f.writelines(lines)
+            std = os.path.join(td, "std")
+            run(REF, cfg, std)
+            outs = {}
+            for fn in sorted(os.listdir(std)):
+                if fn.startswith(("spikes-", "ratesPerPop-")):
+                    outs[fn] = sha256(os.path.join(std, fn))
+            entry["outputs_sha256"] = outs
+            with gzip.open(os.path.join(HERE, f"{name}.spikes.gz"), "wt") as f:
+                with open(os.path.join(std, f"spikes-sec0-C{cfg.n_modules}-H{cfg.glob_h}-h000.dat")) as g:
+                    f.write(g.read())
+        manifest[name] = entry
+        print(name, entry["spikes"], "spikes", flush=True)
+    with open(os.path.join(HERE, "manifest.json"), "w") as f:
+        json.dump(manifest, f, indent=1, sort_keys=True)
+
+
+if __name__ == "__main__":
+    main()
