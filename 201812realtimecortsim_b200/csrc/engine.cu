@@ -331,8 +331,8 @@ __global__ void gen_kernel(const NetConst *__restrict__ net, const float *__rest
       // external bath rate (ModuleGen.cpp:201-211, LIFCAconnectome.cpp:871-887)
       float nu = (float)net->NuExt[ssub];
       uint32_t bx = cfx, by = cfy;
-      if (bx >= net->cfx / 2) bx = -1 * (bx - net->cfx + 1);
-      if (by >= net->cfy / 2) by = -1 * (by - net->cfy + 1);
+      if (bx >= net->cfx / 2) bx = 0u - (bx - net->cfx + 1u);   // unsigned, as the reference computes it
+      if (by >= net->cfy / 2) by = 0u - (by - net->cfy + 1u);
       if (bx >= net->stencil_dim) bx = net->stencil_dim - 1;
       if (by >= net->stencil_dim) by = net->stencil_dim - 1;
       float cext = (float)bath_tmpl[bx * net->stencil_dim + by];
@@ -1259,12 +1259,17 @@ struct dpsnn_engine {
   std::vector<void *> allocs;
   uint32_t grid_neuron = 0, grid_deliver = 0, grid_heavy = 0;
   int timing = 0;
-  cudaEvent_t ev[12];
+  struct TimedLaunch { int family; cudaEvent_t a, b; };
+  std::vector<TimedLaunch> pending;   // recorded, not yet read
+  std::vector<cudaEvent_t> event_pool;
   double ktime[5] = {0, 0, 0, 0, 0};
   uint64_t klaunch[5] = {0, 0, 0, 0, 0};
+  uint64_t launches = 0;               // kernels enqueued by dpsnn_step
   std::vector<float> fix_vals;
   std::vector<uint32_t> fix_keys, fix_bucket;
 };
+
+static void collect_timings(dpsnn_engine *e);
 
 template <typename T>
 static int dalloc(dpsnn_engine *e, T **p, size_t n, bool zero = true) {
@@ -1767,7 +1772,6 @@ extern "C" int dpsnn_create(const dpsnn_params *p, const dpsnn_options *opts, dp
     delete e;
     return dpsnn_fail(DPSNN_E_CUDA, "cannot set up device %d", e->device);
   }
-  for (int k = 0; k < 12; k++) cudaEventCreate(&e->ev[k]);
   int rc = engine_build(e, p, opts);
   if (rc) {
     dpsnn_destroy(e);
@@ -1782,7 +1786,8 @@ extern "C" void dpsnn_destroy(dpsnn_engine *e) {
   cudaSetDevice(e->device);
   if (e->stream) cudaStreamSynchronize(e->stream);
   for (void *q : e->allocs) cudaFree(q);
-  for (int k = 0; k < 12; k++) cudaEventDestroy(e->ev[k]);
+  collect_timings(e);
+  for (cudaEvent_t ev : e->event_pool) cudaEventDestroy(ev);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
 }
@@ -1801,18 +1806,43 @@ static int check_flags(dpsnn_engine *e) {
   return dpsnn_fail(DPSNN_E_MODEL, "device error flags 0x%x", f);
 }
 
+// Kernel timing records an event pair per kernel family and step on the
+// engine stream without synchronising; dpsnn_kernel_times reads them.
+static cudaEvent_t pool_event(dpsnn_engine *e) {
+  if (e->event_pool.empty()) {
+    cudaEvent_t ev;
+    cudaEventCreate(&ev);
+    return ev;
+  }
+  cudaEvent_t ev = e->event_pool.back();
+  e->event_pool.pop_back();
+  return ev;
+}
 static void timed_launch_begin(dpsnn_engine *e, int k) {
-  if (e->timing) cudaEventRecord(e->ev[2 * k], e->stream);
+  if (!e->timing) return;
+  dpsnn_engine::TimedLaunch tl;
+  tl.family = k;
+  tl.a = pool_event(e);
+  tl.b = pool_event(e);
+  cudaEventRecord(tl.a, e->stream);
+  e->pending.push_back(tl);
 }
 static void timed_launch_end(dpsnn_engine *e, int k) {
-  if (e->timing) {
-    cudaEventRecord(e->ev[2 * k + 1], e->stream);
-    cudaEventSynchronize(e->ev[2 * k + 1]);
+  if (!e->timing) return;
+  (void)k;
+  cudaEventRecord(e->pending.back().b, e->stream);
+}
+static void collect_timings(dpsnn_engine *e) {
+  for (auto &tl : e->pending) {
+    cudaEventSynchronize(tl.b);
     float ms = 0;
-    cudaEventElapsedTime(&ms, e->ev[2 * k], e->ev[2 * k + 1]);
-    e->ktime[k] += ms * 1e-3;
-    e->klaunch[k]++;
+    cudaEventElapsedTime(&ms, tl.a, tl.b);
+    e->ktime[tl.family] += ms * 1e-3;
+    e->klaunch[tl.family]++;
+    e->event_pool.push_back(tl.a);
+    e->event_pool.push_back(tl.b);
   }
+  e->pending.clear();
 }
 
 static int enqueue_step(dpsnn_engine *e) {
@@ -1843,6 +1873,7 @@ static int enqueue_step(dpsnn_engine *e) {
     timed_launch_end(e, 4);
   }
   end_step_kernel<<<1, 1, 0, e->stream>>>(d);
+  e->launches += 8 + (e->hnet.stdp_on ? 2 : 0);
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) return dpsnn_fail(DPSNN_E_CUDA, "kernel launch: %s", cudaGetErrorString(err));
   e->t_host++;
@@ -1989,8 +2020,13 @@ extern "C" int dpsnn_set_timing(dpsnn_engine *e, int enable) {
   return 0;
 }
 
+extern "C" uint64_t dpsnn_kernel_launches(const dpsnn_engine *e) { return e ? e->launches : 0; }
+extern "C" void *dpsnn_cuda_stream(const dpsnn_engine *e) { return e ? (void *)e->stream : nullptr; }
+
 extern "C" int dpsnn_kernel_times(dpsnn_engine *e, double *seconds5, uint64_t *launches5) {
   if (!e) return dpsnn_fail(DPSNN_E_PARAM, "null engine");
+  cudaSetDevice(e->device);
+  collect_timings(e);
   for (int k = 0; k < 5; k++) {
     if (seconds5) seconds5[k] = e->ktime[k];
     if (launches5) launches5[k] = e->klaunch[k];

@@ -53,7 +53,7 @@ EXPORTS = [
     "dpsnn_params_from_env", "dpsnn_create", "dpsnn_destroy", "dpsnn_step", "dpsnn_sync",
     "dpsnn_glob_n", "dpsnn_time_ms", "dpsnn_synapse_count", "dpsnn_events_delivered",
     "dpsnn_spikes", "dpsnn_rank_synapse_count", "dpsnn_backward_synapses", "dpsnn_state",
-    "dpsnn_bath_params", "dpsnn_set_timing", "dpsnn_kernel_times", "dpsnn_last_error",
+    "dpsnn_bath_params", "dpsnn_set_timing", "dpsnn_kernel_times", "dpsnn_kernel_launches", "dpsnn_cuda_stream", "dpsnn_last_error",
 ]
 
 _LIB = None
@@ -90,6 +90,10 @@ def load_library(path: str = LIB_PATH):
     lib.dpsnn_bath_params.argtypes = [P, P, P]
     lib.dpsnn_set_timing.argtypes = [P, C.c_int]
     lib.dpsnn_kernel_times.argtypes = [P, P, P]
+    lib.dpsnn_kernel_launches.argtypes = [P]
+    lib.dpsnn_kernel_launches.restype = C.c_uint64
+    lib.dpsnn_cuda_stream.argtypes = [P]
+    lib.dpsnn_cuda_stream.restype = C.c_void_p
     lib.dpsnn_last_error.restype = C.c_char_p
     _LIB = lib
     return lib
@@ -235,6 +239,12 @@ class Engine:
 
     def set_timing(self, on: bool):
         self._check(self._L.dpsnn_set_timing(self._h, 1 if on else 0), "dpsnn_set_timing")
+
+    def cuda_stream(self) -> int:
+        return self._L.dpsnn_cuda_stream(self._h)
+
+    def kernel_launches(self) -> int:
+        return self._L.dpsnn_kernel_launches(self._h)
 
     def kernel_times(self):
         sec = np.zeros(5, np.float64)

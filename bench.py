@@ -1,0 +1,344 @@
+"""Benchmark: synaptic events/s of DPSNN's per-timestep loop on the 24x24 grid.
+
+One bench step is one 1 ms simulation step of the 24x24 cortical-module grid
+(720000 neurons, ~0.81 G synapses, 10 s network; STDP off) -- synapse
+delivery, Poisson bath, LIFCA update and spike compaction for the whole grid,
+with the RNG streams of 192 reference ranks (env_globH=192, the largest
+reference decomposition of this grid: 3 modules per rank).  The network lives
+in HBM; the timed region covers K consecutive steps after W warm-up steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+value  = synaptic events delivered in the K steps / device time (CUDA events
+         on the engine stream), summed over ranks (independent replicas).
+e2e    = the same metric through the C ABI as a drop-in caller uses it: one
+         dpsnn_step per ms and the step's spike list read back to host memory
+         (the raster), timed on the host; no per-step input goes to the device.
+The reference arm (--impl reference) runs the reference binary built from the
+reference sources (oracle/_ref/dpsnn_ref) on the host cores: one single-rank
+process per core, each simulating the 2x2 network (the reference's
+CPU-runnable case: 5000 neurons, ~5.6 M synapses, 1 s), events counted by the
+committed fixture of that run.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "synaptic events/s"
+UNIT = "events/s"
+WORKLOAD = "24x24 grid, 720000 neurons, ~0.81G synapses, 1 ms steps, STDP off, RNG streams of 192 ranks"
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.out,
+                stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        self.out.flush()
+        self.out.seek(0)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl" if args.impl == "b200" else "gloo",
+                                timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+FIRE_RE = re.compile(r"total fire time = ([0-9.eE+-]+)")
+
+
+def reference_c1_start(workdir: str, binary: str):
+    """Start the reference binary on the 2x2 grid (1000 ms, 1 rank) in
+    ``workdir``; the caller waits and parses its output."""
+    nc = importlib.import_module("201812realtimecortsim_b200.netconfig")
+    cfg = nc.cortical_grid(2, 2, total_ms=1000)
+    os.makedirs(workdir, exist_ok=True)
+    env = dict(os.environ)
+    env.update(cfg.write(workdir))
+    return subprocess.Popen([binary], cwd=workdir, env=env, stdout=subprocess.PIPE,
+                            stderr=subprocess.DEVNULL, text=True)
+
+
+def reference_fire_seconds(proc) -> float:
+    """Time the reference spent in localNetProcess_fire (its own CHRONO line:
+    the 1001 simulation steps, connectome construction excluded)."""
+    out, _ = proc.communicate()
+    if proc.returncode != 0:
+        raise RuntimeError("reference run failed")
+    m = FIRE_RE.search(out)
+    if not m:
+        raise RuntimeError("reference output has no fire time")
+    return float(m.group(1))
+
+
+def reference_events_c1() -> int:
+    with open(os.path.join(ROOT, "tests", "golden", "manifest.json")) as f:
+        return int(json.load(f)["c1_2x2"]["events"])
+
+
+def reference_processes() -> int:
+    """One reference process per host thread, bounded by host memory
+    (about 0.4 GB resident per process)."""
+    n = os.cpu_count() or 1
+    try:
+        import psutil
+        n = min(n, max(1, int(psutil.virtual_memory().available / 1.0e9)))
+    except Exception:
+        pass
+    return n
+
+
+def run_reference(args, world, rank):
+    """Reference arm: the reference binary built from its sources, one
+    single-rank process per host thread, each simulating 1000 ms of the 2x2
+    grid; a bench step is one such batch (at most 2 batches are timed)."""
+    if rank != 0:
+        return
+    binary = os.path.join(ROOT, "oracle", "_ref", "dpsnn_ref")
+    if not os.path.exists(binary):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/dpsnn_ref was not built"}))
+        return
+    cores = reference_processes()
+    events = reference_events_c1()
+    batches = max(1, min(args.steps, 2))
+    rates, walls = [], []
+    for it in range(batches):
+        with tempfile.TemporaryDirectory() as td:
+            t0 = time.perf_counter()
+            procs = [reference_c1_start(os.path.join(td, f"r{c}"), binary) for c in range(cores)]
+            fire = [reference_fire_seconds(p) for p in procs]
+            walls.append(time.perf_counter() - t0)
+        rates.append(sum(events / f for f in fire))
+    value = statistics.mean(rates)
+    sample = (f"reference binary, 2x2 grid (5000 neurons, 5.6M synapses), 1000 ms per process, "
+              f"{cores} concurrent processes, {batches} batch(es); time = its own fire() CHRONO")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": batches, "warmup": 0, "ms_per_step": 1e3 * statistics.mean(walls),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: network generated by the reference's own generator, seed 1",
+        "config": {"workload": "2x2 grid, 5000 neurons, 1 ms steps, STDP off, 1 rank per process "
+                               "(the reference's CPU-runnable case; the 24x24 grid needs 192 MPI ranks)",
+                   "parallelism": f"{cores} processes"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--e2e-steps", type=int, default=300)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local, dist = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    import torch
+    E = importlib.import_module("201812realtimecortsim_b200.engine")
+    nc = importlib.import_module("201812realtimecortsim_b200.netconfig")
+    torch.cuda.set_device(local)
+    prof_steps = min(200, args.steps)
+    total_ms = max(10000, args.warmup + args.steps + prof_steps + args.e2e_steps + 10)
+    cfg = nc.cortical_grid(24, 24, total_ms=total_ms, glob_h=192)
+    eng = E.Engine(cfg, device=local)
+    eng.step(args.warmup)
+    eng.sync()
+    stream = torch.cuda.ExternalStream(eng.cuda_stream())
+
+    def all_max(x):
+        if not dist:
+            return x
+        t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def all_sum(x):
+        if not dist:
+            return x
+        t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t)
+        return float(t.item())
+
+    # timed region: K steps, device time on the engine stream
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0 = eng.events_delivered()
+    l0 = eng.kernel_launches()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        eng.step(args.steps)
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    eng.sync()
+    elapsed = ev0.elapsed_time(ev1) * 1e-3
+    events = eng.events_delivered() - e0
+    launches = eng.kernel_launches() - l0
+    t_max = all_max(elapsed)
+    ev_tot = all_sum(events)
+
+    # per-kernel-family device times over the following steps (event pairs
+    # around each family; kept out of the timed region above)
+    eng.set_timing(True)
+    p0 = eng.events_delivered()
+    eng.step(prof_steps)
+    eng.sync()
+    eng.set_timing(False)
+    ksec, kcnt = eng.kernel_times()
+    prof_events = eng.events_delivered() - p0
+
+    # e2e: step by step through the C ABI, each step's spikes read back to host
+    t_e = eng.time_ms
+    d2h = 0
+    ee0 = eng.events_delivered()
+    if dist:
+        dist.barrier()
+    h0 = time.perf_counter()
+    for k in range(args.e2e_steps):
+        eng.step(1)
+        ids, te = eng.spikes(t_e + k)
+        d2h += ids.nbytes + te.nbytes + 4
+    h1 = time.perf_counter()
+    e2e_events = eng.events_delivered() - ee0
+    e2e_val = all_sum(e2e_events) / all_max(h1 - h0)
+
+    hbm, peak_kind = peaks()
+    fam = ["compact", "deliver", "bath", "neuron", "plasticity"]
+    fam_total = float(sum(ksec)) or 1.0
+    kernel_share = {f: float(s) / fam_total for f, s in zip(fam, ksec)}
+    kernel_ms = {f: (1e3 * float(s) / int(c) if c else 0.0) for f, s, c in zip(fam, ksec, kcnt)}
+    # delivery kernel: per synaptic event it reads the u32 target and the
+    # i16 weight of the synapse and writes one 8-byte {key, weight} record
+    deliver_s = float(ksec[1]) / max(int(kcnt[1]), 1)
+    ev_per_launch = prof_events / max(int(kcnt[1]), 1)
+    achieved = 14.0 * ev_per_launch / deliver_s / 1e9 if deliver_s > 0 else 0.0
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "deliver_traffic.json")
+    if os.path.exists(tfile):
+        with open(tfile) as f:
+            traffic = float(json.load(f)["dram_bytes_per_event"]) * ev_per_launch
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        binary = os.path.join(ROOT, "oracle", "_ref", "dpsnn_ref")
+        if os.path.exists(binary):
+            with tempfile.TemporaryDirectory() as td:
+                fire = reference_fire_seconds(reference_c1_start(td, binary))
+            cpu = {"value": reference_events_c1() / fire, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"reference binary, 2x2 grid (5000 neurons, 5.6M synapses), 1000 ms, 1 rank, "
+                             f"{fire:.1f} s in fire()"}
+    if rank == 0:
+        clocks = clk.summary()
+        out = {
+            "metric": METRIC, "value": ev_tot / t_max, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: network generated by the reference's algorithm, seed 1",
+            "config": {"workload": WORKLOAD, "global_batch": world, "seq_len": args.steps,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (connectome ~5 GB read every step)",
+                       "real_time_factor": t_max / (args.steps * 1e-3),
+                       "events_per_step": events / args.steps},
+            "roofline": {"bound": "hbm", "kernel": "deliver_kernel", "achieved": achieved, "peak": hbm,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": traffic, "algorithmic_bytes_per_event": 14,
+                         "events_per_launch": ev_per_launch},
+            "kernel_ms": kernel_ms,
+            "kernel_share": kernel_share,
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": d2h / max(args.e2e_steps, 1), "steps": args.e2e_steps},
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(out))
+    eng.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -135,9 +135,15 @@ int dpsnn_bath_params(dpsnn_engine *e, double *inv_nu_ext, uint32_t *max_ext);
 
 /* Seconds of device time spent in each kernel family since creation
  * (index: 0 compaction, 1 delivery, 2 bath, 3 neuron update, 4 plasticity);
- * filled only when timing was enabled with dpsnn_set_timing(e, 1). */
+ * counted only while timing is enabled with dpsnn_set_timing(e, 1), which
+ * records CUDA events around each family without synchronising. */
 int dpsnn_set_timing(dpsnn_engine *e, int enable);
 int dpsnn_kernel_times(dpsnn_engine *e, double *seconds5, uint64_t *launches5);
+/* Kernels enqueued by dpsnn_step since creation. */
+uint64_t dpsnn_kernel_launches(const dpsnn_engine *e);
+/* The cudaStream_t all of the engine's work is enqueued on (for timing
+ * with CUDA events by the caller). */
+void *dpsnn_cuda_stream(const dpsnn_engine *e);
 
 const char *dpsnn_last_error(void);
 

@@ -11,7 +11,8 @@ built from the unmodified sources plus the bounds fix:
 * ``<case>.raster.gz``   full-precision raster (%.17g) of the reference;
 * ``<case>.spikes.gz``   the reference's own spikes file (%.7g);
 * ``manifest.json``      sha256 of the BACKWARD synapse dump and of the
-                          output files, spike counts, configuration.
+                          output files, spike and synaptic-event counts,
+                          configuration.
 
 Usage: python tests/golden/make_golden.py
 """
@@ -86,6 +87,16 @@ def main():
             with gzip.open(os.path.join(HERE, f"{name}.spikes.gz"), "wt") as f:
                 with open(os.path.join(std, f"spikes-sec0-C{cfg.n_modules}-H{cfg.glob_h}-h000.dat")) as g:
                     f.write(g.read())
+        # synaptic events delivered in the run (identical dynamics in the
+        # restatement, pinned by the raster and dump checks)
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import dpsnn_oracle as O
+        net = O.OracleNet(cfg)
+        ev = 0
+        for _ in range(cfg.total_ms):
+            net.step()
+            ev += net.last_event_count()
+        entry["events"] = ev
         manifest[name] = entry
         print(name, entry["spikes"], "spikes", flush=True)
     with open(os.path.join(HERE, "manifest.json"), "w") as f:
