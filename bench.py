@@ -126,6 +126,12 @@ def reference_c1_start(workdir: str, binary: str):
     os.makedirs(workdir, exist_ok=True)
     env = dict(os.environ)
     env.update(cfg.write(workdir))
+    # the reference's own switches for its raster and rate files: off, so
+    # that its timed loop does no file output (the engine's loop does none)
+    env["env_spikes_writeDisable"] = "1"
+    env["env_statRatesPerPop_writeDisable"] = "1"
+    # its 185 MB synapse-list text dump at init goes to /dev/null
+    os.symlink(os.devnull, os.path.join(workdir, f"localNet_h0_N{cfg.glob_n}_SynapticList_BACKWARD_R-1.dat"))
     return subprocess.Popen([binary], cwd=workdir, env=env, stdout=subprocess.PIPE,
                             stderr=subprocess.DEVNULL, text=True)
 
