@@ -1,0 +1,253 @@
+// localnet.cpp -- the DAL process trio of DPSNN over the B200 engine, and
+// the reference's per-rank output files (spikes, ratesPerPop,
+// FiringsInChronoWindow) written from the engine's spike lists.
+//
+// Output formats restate DPSNN_stat.c (file names :66-83, spikes :290-308,
+// ratesPerPop :227-275, open/close windows :594-745) and
+// DPSNN_localNet_sim.c (per-population counts :229-253, chrono window
+// statistics :1001-1036).  The stopWatch semantics are those of
+// DPSNN_stopWatch.c:15-44.
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "dpsnn_b200.h"
+#include "dpsnn_localnet.h"
+
+namespace {
+
+[[noreturn]] void die(const char *what) {
+  printf("ERROR %s: %s\n", what, dpsnn_last_error());
+  fflush(stdout);
+  exit(0);  // the reference exits with status 0 on every error
+}
+
+// One emulated rank's stat files and chrono-window counters.
+struct RankStat {
+  FILE *spikes = nullptr, *rates = nullptr;
+  std::vector<uint32_t> per_pop;   // N_firingsPerPop (globCFT*nsub entries)
+  uint32_t n_win = 0, min_win = (uint32_t)-1, max_win = 0, laps = 0;
+  double mean = 0, var = 0, sigma = 0, cv = 0, m2 = 0;
+};
+
+struct LocalNet {
+  dpsnn_params par;
+  dpsnn_engine *eng = nullptr;
+  int32_t ms = 0, max_ms = 0;
+  uint32_t P = 1, locN = 0, npcm = 0, globCFT = 0;
+  float locCFT = 1.0f;
+  uint32_t chrono = 0, chrono_start = 0, chrono_stop = 0;
+  std::vector<RankStat> rank;
+  std::vector<uint32_t> ids;
+  std::vector<double> te;
+};
+
+LocalNet *g_net = nullptr;
+
+bool stat_second(const dpsnn_params &p, uint32_t sec) {
+  return sec >= p.startStatFiles_s && sec <= p.stopStatFiles_s && sec % p.moduloSec == 0;
+}
+bool rates_second(const dpsnn_params &p, uint32_t sec) {
+  return stat_second(p, sec) && sec >= p.startRatesPerPop_s && sec <= p.stopRatesPerPop_s;
+}
+
+FILE *open_stat(const LocalNet &n, const char *prefix, uint32_t sec, uint32_t h) {
+  char name[320];
+  if (n.par.howManyOutputFiles == 1) {
+    snprintf(name, sizeof name, "%s-sec%u-C%u-H%u-h%03u.dat", prefix, sec, n.globCFT, n.P, h);
+  } else if (sec == 0) {
+    snprintf(name, sizeof name, "%s-start-C%u-H%u-h%u.dat", prefix, n.globCFT, n.P, h);
+  } else if (sec % 2 == 0) {
+    snprintf(name, sizeof name, "%s-lasteven-C%u-H%u-h%u.dat", prefix, n.globCFT, n.P, h);
+  } else {
+    snprintf(name, sizeof name, "%s-lastodd-C%u-H%u-h%u.dat", prefix, n.globCFT, n.P, h);
+  }
+  FILE *f = fopen(name, "w");
+  if (!f) {
+    printf("ERROR NULL fp\n");
+    fflush(stdout);
+    exit(0);
+  }
+  return f;
+}
+
+void close_stat(FILE *&f) {
+  if (f && fclose(f) != 0) {
+    printf("ERROR fclose!=0 in stat_sfclose\n");
+    fflush(stdout);
+    exit(0);
+  }
+  f = nullptr;
+}
+
+void open_second(LocalNet &n, uint32_t sec) {
+  for (uint32_t h = 0; h < n.P; h++) {
+    RankStat &r = n.rank[h];
+    if (!n.par.spikes_writeDisable && stat_second(n.par, sec)) r.spikes = open_stat(n, "spikes", sec, h);
+    if (!n.par.statRatesPerPop_writeDisable && rates_second(n.par, sec))
+      r.rates = open_stat(n, "ratesPerPop", sec, h);
+  }
+}
+
+void close_second(LocalNet &n) {
+  for (RankStat &r : n.rank) {
+    close_stat(r.spikes);
+    close_stat(r.rates);
+  }
+}
+
+uint32_t subpop_in_module(const dpsnn_params &p, uint32_t in_cm) {
+  uint32_t s = 0;
+  while (s < p.nsub) {
+    if (in_cm < p.count[s]) break;
+    in_cm -= p.count[s];
+    s++;
+  }
+  return s;
+}
+
+// The per-step outputs of one rank: its spike lines, its per-population
+// counts and, every ratesSampling ms, its rate line; then the chrono window.
+void rank_outputs(LocalNet &n, uint32_t h, const uint32_t *ids, const double *te, uint32_t cnt) {
+  const dpsnn_params &p = n.par;
+  RankStat &r = n.rank[h];
+  const uint32_t ms = (uint32_t)n.ms;
+  if (r.spikes)
+    for (uint32_t i = 0; i < cnt; i++) {
+      fprintf(r.spikes, "%d %.7g\n", (int)ids[i], te[i]);
+      fflush(r.spikes);
+    }
+  const uint32_t first_pop = (h * n.locN / n.npcm) * p.nsub;
+  for (uint32_t i = 0; i < cnt; i++) {
+    const uint32_t col = ids[i] / n.npcm;
+    const uint32_t pop = col * p.nsub + subpop_in_module(p, ids[i] - col * n.npcm);
+    r.per_pop[pop - first_pop]++;
+  }
+  if (r.rates && ms % p.ratesSampling == 0) {
+    fprintf(r.rates, "%d ", (int)(ms - p.ratesSampling));
+    for (uint32_t tot = 0; (float)tot < n.locCFT * (float)p.nsub; tot += p.nsub)
+      for (uint32_t s = 0; s < p.nsub; s++)
+        fprintf(r.rates, "%.7g ",
+                ((float)(r.per_pop[tot + s]) * 1000.0) / ((float)(p.count[s]) * (float)(p.ratesSampling)));
+    fprintf(r.rates, " \n");
+    fflush(r.rates);
+    std::fill(r.per_pop.begin(), r.per_pop.end(), 0u);
+  }
+  if (ms >= n.chrono_start && ms < n.chrono_stop) {
+    r.n_win += cnt;
+    r.laps++;
+    r.min_win = cnt < r.min_win ? cnt : r.min_win;
+    r.max_win = cnt > r.max_win ? cnt : r.max_win;
+    const double delta = cnt - r.mean;
+    r.mean += (double)(delta / r.laps);
+    r.m2 += (double)((double)delta * (double)((double)cnt - (double)r.mean));
+    r.var = (double)(r.m2 / (r.laps - 1));
+    r.sigma = (double)(sqrt(r.var));
+    r.cv = (double)(r.sigma / r.mean);
+  }
+}
+
+void write_chrono_window(const LocalNet &n, uint32_t h) {
+  const RankStat &r = n.rank[h];
+  char name[80];
+  snprintf(name, sizeof name, "FiringsInChronoWindow_h%u.stat", h);
+  FILE *f = fopen(name, "w");
+  if (!f) return;
+  const double rate = double((double)r.n_win * 1000) / double((double)r.laps * (double)n.locN);
+  fprintf(f,
+          "FIRING-h=%.3d     Firings in ms %6d-%6d = %-11d min = %-11d max = %-11d mean = %-11f variance = "
+          "%-11f sigma = %-11f coeffOfVariation = %-11f samples = %d\n",
+          (int)h, (int)n.chrono_start, (int)n.chrono_stop, (int)r.n_win, (int)r.min_win, (int)r.max_win, r.mean,
+          r.var, r.sigma, r.cv, (int)r.laps);
+  fprintf(f, "FIRING-h=%.3d  FiringRate in ms %6d-%6d = %-11f\n", (int)h, (int)n.chrono_start,
+          (int)n.chrono_stop, rate);
+  fclose(f);
+}
+
+uint32_t env_u32_or(const char *name, uint32_t dflt) {
+  const char *s = getenv(name);
+  return s ? (uint32_t)atoi(s) : dflt;
+}
+
+}  // namespace
+
+void localNetProcess_init(DALProcess *p) {
+  (void)p;
+  if (g_net) {
+    printf("ERROR localNetProcess_init called twice\n");
+    fflush(stdout);
+    exit(0);
+  }
+  LocalNet *n = new LocalNet();
+  if (dpsnn_params_from_env(nullptr, &n->par)) die("getParameters");
+  dpsnn_options opt;
+  memset(&opt, 0, sizeof opt);
+  opt.device = (int)env_u32_or("DPSNN_DEVICE", 0);
+  if (dpsnn_create(&n->par, &opt, &n->eng)) die("localNetClass::init");
+  const dpsnn_params &q = n->par;
+  n->P = q.glob_h;
+  n->globCFT = q.cfx * q.cfy;
+  n->npcm = 0;
+  for (uint32_t s = 0; s < q.nsub; s++) n->npcm += q.count[s];
+  n->locN = dpsnn_glob_n(n->eng) / n->P;
+  n->locCFT = ((float)n->globCFT / (float)n->P);
+  n->max_ms = (int32_t)q.total_sim_time_ms;
+  n->chrono = env_u32_or("env_chrono", 0);
+  n->chrono_start = env_u32_or("env_startPartialChrono_ms", 0);
+  n->chrono_stop = n->chrono_start + env_u32_or("env_partialChronoWindow_ms", 0);
+  n->rank.resize(n->P);
+  for (RankStat &r : n->rank) r.per_pop.assign((size_t)n->globCFT * q.nsub, 0u);
+  n->ids.resize(dpsnn_glob_n(n->eng));
+  n->te.resize(dpsnn_glob_n(n->eng));
+  g_net = n;
+}
+
+int localNetProcess_fire(DALProcess *p) {
+  (void)p;
+  LocalNet *n = g_net;
+  if (!n) {
+    printf("ERROR localNetProcess_fire before init\n");
+    fflush(stdout);
+    exit(0);
+  }
+  if (n->ms > n->max_ms) {
+    printf("ERROR programmed max sim time ms exceeded\n");
+    exit(0);
+  }
+  if (n->ms == n->max_ms) return 1;
+  const uint32_t sec = (uint32_t)n->ms / 1000;
+  if (n->ms % 1000 == 0) open_second(*n, sec);
+  if (dpsnn_step(n->eng, 1)) die("completeTimeStep_ms");
+  uint32_t cnt = 0;
+  if (dpsnn_spikes(n->eng, (uint32_t)n->ms, n->ids.data(), n->te.data(), (uint32_t)n->ids.size(), &cnt))
+    die("completeTimeStep_ms");
+  // the list is rank-major and ascending: split it at the rank boundaries
+  uint32_t a = 0;
+  for (uint32_t h = 0; h < n->P; h++) {
+    const uint32_t end_id = (h + 1) * n->locN;
+    uint32_t b = a;
+    while (b < cnt && n->ids[b] < end_id) b++;
+    rank_outputs(*n, h, n->ids.data() + a, n->te.data() + a, b - a);
+    a = b;
+  }
+  if (n->ms % 1000 == 999) close_second(*n);
+  n->ms++;
+  return 0;
+}
+
+void localNetProcess_finish(DALProcess *p) {
+  (void)p;
+  LocalNet *n = g_net;
+  if (!n) return;
+  if (n->chrono == 1)
+    for (uint32_t h = 0; h < n->P; h++) write_chrono_window(*n, h);
+  close_second(*n);
+  dpsnn_destroy(n->eng);
+  delete n;
+  g_net = nullptr;
+}
+
+struct dpsnn_engine *localNetProcess_engine(void) { return g_net ? g_net->eng : nullptr; }

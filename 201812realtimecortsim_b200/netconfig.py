@@ -118,6 +118,8 @@ class NetConfig:
             "env_CFY": str(self.cfy),
             "env_D": str(self.D),
             "env_chrono": "1",
+            "env_startPartialChrono_ms": "0",
+            "env_partialChronoWindow_ms": str(self.total_ms),
             "env_totalSimTime_ms": str(self.total_ms),
             "env_startPlasticity_ms": str(self.start_plasticity_ms),
             "env_stopPlasticity_ms": str(self.stop_plasticity_ms),

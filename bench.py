@@ -207,7 +207,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
-    ap.add_argument("--e2e-steps", type=int, default=300)
+    ap.add_argument("--e2e-steps", type=int, default=0, help="0 = the same K steps as the timed region")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -276,20 +276,28 @@ def main():
     ksec, kcnt = eng.kernel_times()
     prof_events = eng.events_delivered() - p0
 
-    # e2e: step by step through the C ABI, each step's spikes read back to host
-    t_e = eng.time_ms
+    eng.close()
+
+    # e2e: the same steps W..W+K-1 of the same network (the simulation is
+    # deterministic), stepped one at a time through the C ABI with each
+    # step's spike list read back to host memory, timed on the host
+    eng = E.Engine(cfg, device=local)
+    eng.step(args.warmup)
+    eng.sync()
+    e2e_steps = args.steps if args.e2e_steps <= 0 else min(args.e2e_steps, args.steps)
     d2h = 0
     ee0 = eng.events_delivered()
     if dist:
         dist.barrier()
     h0 = time.perf_counter()
-    for k in range(args.e2e_steps):
+    for k in range(e2e_steps):
         eng.step(1)
-        ids, te = eng.spikes(t_e + k)
+        ids, te = eng.spikes(args.warmup + k)
         d2h += ids.nbytes + te.nbytes + 4
     h1 = time.perf_counter()
     e2e_events = eng.events_delivered() - ee0
     e2e_val = all_sum(e2e_events) / all_max(h1 - h0)
+    eng.close()
 
     hbm, peak_kind = peaks()
     fam = ["compact", "deliver", "bath", "neuron", "plasticity"]
@@ -334,7 +342,8 @@ def main():
             "kernel_ms": kernel_ms,
             "kernel_share": kernel_share,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": d2h / max(args.e2e_steps, 1), "steps": args.e2e_steps},
+                    "d2h_bytes_per_step": d2h / max(e2e_steps, 1), "steps": e2e_steps,
+                    "ms_per_step": 1e3 * (h1 - h0) / max(e2e_steps, 1)},
             "gpu_launches": launches,
             "clocks": clocks,
             "cpu_baseline": cpu,

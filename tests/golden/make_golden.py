@@ -11,14 +11,16 @@ built from the unmodified sources plus the bounds fix:
 * ``<case>.raster.gz``   full-precision raster (%.17g) of the reference;
 * ``<case>.spikes.gz``   the reference's own spikes file (%.7g);
 * ``manifest.json``      sha256 of the BACKWARD synapse dump and of the
-                          output files, spike and synaptic-event counts,
-                          configuration.
+                          output files (spikes, ratesPerPop,
+                          FiringsInChronoWindow), spike and synaptic-event
+                          counts, configuration.
 
 Usage: python tests/golden/make_golden.py
 """
 import gzip
 import hashlib
 import importlib
+import io
 import json
 import os
 import shutil
@@ -43,6 +45,11 @@ def sha256(path):
         for chunk in iter(lambda: f.read(1 << 20), b""):
             h.update(chunk)
     return h.hexdigest()
+
+
+def gz_text(path):
+    """Text writer of a gzip file with no timestamp (byte-stable output)."""
+    return io.TextIOWrapper(gzip.GzipFile(path, "wb", mtime=0))
 
 
 def run(binary, cfg, workdir):
@@ -75,16 +82,16 @@ def main():
                     with open(fn) as f:
                         lines += f.readlines()
             entry["spikes"] = len(lines)
-            with gzip.open(os.path.join(HERE, f"{name}.raster.gz"), "wt") as f:
+            with gz_text(os.path.join(HERE, f"{name}.raster.gz")) as f:
                 f.writelines(lines)
             std = os.path.join(td, "std")
             run(REF, cfg, std)
             outs = {}
             for fn in sorted(os.listdir(std)):
-                if fn.startswith(("spikes-", "ratesPerPop-")):
+                if fn.startswith(("spikes-", "ratesPerPop-", "FiringsInChronoWindow_")):
                     outs[fn] = sha256(os.path.join(std, fn))
             entry["outputs_sha256"] = outs
-            with gzip.open(os.path.join(HERE, f"{name}.spikes.gz"), "wt") as f:
+            with gz_text(os.path.join(HERE, f"{name}.spikes.gz")) as f:
                 with open(os.path.join(std, f"spikes-sec0-C{cfg.n_modules}-H{cfg.glob_h}-h000.dat")) as g:
                     f.write(g.read())
         # synaptic events delivered in the run (identical dynamics in the

@@ -24,6 +24,15 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_localnet_exports_the_dal_trio_with_cxx_linkage():
+    """libdpsnn_localnet.so defines the three symbols the reference's MPI
+    main leaves undefined (C++ names of localNetProcess.h:72-74)."""
+    lib = C.CDLL(os.path.join(ROOT, "201812realtimecortsim_b200", "libdpsnn_localnet.so"))
+    for sym in ("_Z20localNetProcess_initP8_process", "_Z20localNetProcess_fireP8_process",
+                "_Z22localNetProcess_finishP8_process"):
+        assert hasattr(lib, sym), sym
+
+
 def test_binding_covers_the_header():
     assert set(declared_functions()) <= set(E.EXPORTS)
 
