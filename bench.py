@@ -210,6 +210,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=0, help="0 = the same K steps as the timed region")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", default="24x24", help="CFXxCFY modules (profiling of smaller grids)")
+    ap.add_argument("--ranks", type=int, default=192, help="env_globH: emulated reference ranks")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local, dist = dist_setup(args)
@@ -226,7 +228,10 @@ def main():
     torch.cuda.set_device(local)
     prof_steps = min(200, args.steps)
     total_ms = max(10000, args.warmup + args.steps + prof_steps + args.e2e_steps + 10)
-    cfg = nc.cortical_grid(24, 24, total_ms=total_ms, glob_h=192)
+    cfx, cfy = (int(x) for x in args.grid.lower().split("x"))
+    cfg = nc.cortical_grid(cfx, cfy, total_ms=total_ms, glob_h=args.ranks)
+    workload = WORKLOAD if (cfx, cfy, args.ranks) == (24, 24, 192) else (
+        f"{cfx}x{cfy} grid, {cfg.glob_n} neurons, 1 ms steps, STDP off, RNG streams of {args.ranks} ranks")
     eng = E.Engine(cfg, device=local)
     eng.step(args.warmup)
     eng.sync()
@@ -330,7 +335,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic: network generated by the reference's algorithm, seed 1",
-            "config": {"workload": WORKLOAD, "global_batch": world, "seq_len": args.steps,
+            "config": {"workload": workload, "global_batch": world, "seq_len": args.steps,
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (connectome ~5 GB read every step)",
                        "real_time_factor": t_max / (args.steps * 1e-3),
