@@ -26,6 +26,7 @@
 #include <cstring>
 #include <dlfcn.h>
 #include <string>
+#include <mutex>
 #include <vector>
 
 #include "dd_math.cuh"
@@ -2031,5 +2032,104 @@ extern "C" int dpsnn_kernel_times(dpsnn_engine *e, double *seconds5, uint64_t *l
     if (seconds5) seconds5[k] = e->ktime[k];
     if (launches5) launches5[k] = e->klaunch[k];
   }
+  return 0;
+}
+
+// ------------------------------------------------------------------ no-allocation rank spike read
+// dpsnn_rank_spikes_noalloc: the spike list of one emulated rank at one step,
+// gathered on the device into a fixed scratch area that is part of the
+// library image (no cudaMalloc/cudaFree on this path), then copied to the
+// caller's host buffers.  The scratch holds DPSNN_NOALLOC_MAX_SPIKES spikes,
+// the reference's largest rank (miniLocN = 32000 neurons) rounded up; ranks
+// with more neurons are rejected.  One scratch per device and process: calls
+// that overlap in time on the same device race on it.
+struct NoAllocScratch {
+  uint32_t count;                            // written by the kernel each call
+  uint32_t pad[63];
+  uint32_t ids[DPSNN_NOALLOC_MAX_SPIKES];
+  double te[DPSNN_NOALLOC_MAX_SPIKES];
+};
+static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
+
+// One block: binary search of the rank's neuron range [lo, hi) in the
+// ascending spike list of the slot, then an ordered copy of that range.
+// Nothing in the scratch has to start at zero: count and the copied entries
+// are all written here before the host reads them.
+__global__ void rank_select_kernel(const uint32_t *__restrict__ ids, const double *__restrict__ te,
+                                   const uint32_t *__restrict__ cnt_ptr, uint32_t lo, uint32_t hi,
+                                   NoAllocScratch *__restrict__ out) {
+  __shared__ uint32_t s_a, s_b;
+  const uint32_t cnt = *cnt_ptr;
+  if (threadIdx.x == 0) {
+    uint32_t a = 0, b = cnt;
+    while (a < b) {
+      const uint32_t m = (a + b) >> 1;
+      if (ids[m] < lo) a = m + 1; else b = m;
+    }
+    uint32_t c = a, d = cnt;
+    while (c < d) {
+      const uint32_t m = (c + d) >> 1;
+      if (ids[m] < hi) c = m + 1; else d = m;
+    }
+    s_a = a;
+    s_b = c;
+    out->count = c - a;
+  }
+  __syncthreads();
+  const uint32_t a = s_a, n = min(s_b - s_a, (uint32_t)DPSNN_NOALLOC_MAX_SPIKES);
+  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) {
+    out->ids[k] = ids[a + k];
+    out->te[k] = te[a + k];
+  }
+}
+
+#define DPSNN_NOALLOC_MAX_DEVICES 64
+static std::mutex g_noalloc_mu;
+static NoAllocScratch *g_noalloc_addr[DPSNN_NOALLOC_MAX_DEVICES];
+
+// Device address of the scratch, looked up once per device.
+static int noalloc_scratch(int device, NoAllocScratch **out) {
+  if (device < 0 || device >= DPSNN_NOALLOC_MAX_DEVICES)
+    return dpsnn_fail(DPSNN_E_PARAM, "device %d out of range", device);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[device]) {
+    void *p = nullptr;
+    cudaError_t err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (err != cudaSuccess)
+      return dpsnn_fail(DPSNN_E_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(err));
+    g_noalloc_addr[device] = (NoAllocScratch *)p;
+  }
+  *out = g_noalloc_addr[device];
+  return 0;
+}
+
+extern "C" int dpsnn_rank_spikes_noalloc(dpsnn_engine *e, uint32_t t_ms, uint32_t h, uint32_t *ids, double *te,
+                                         uint32_t cap, uint32_t *count) {
+  if (!e || !count) return dpsnn_fail(DPSNN_E_PARAM, "null argument");
+  if (h >= e->hnet.P) return dpsnn_fail(DPSNN_E_PARAM, "rank %u out of range (env_globH = %u)", h, e->hnet.P);
+  if (e->hnet.locN > DPSNN_NOALLOC_MAX_SPIKES)
+    return dpsnn_fail(DPSNN_E_CAPACITY, "rank of %u neurons exceeds the %d-spike scratch of dpsnn_rank_spikes_noalloc",
+                      e->hnet.locN, DPSNN_NOALLOC_MAX_SPIKES);
+  cudaSetDevice(e->device);
+  int rc = dpsnn_sync(e);
+  if (rc) return rc;
+  if (t_ms >= e->t_host || t_ms + RING_SLOTS <= e->t_host)
+    return dpsnn_fail(DPSNN_E_STATE, "step %u is not among the last %d completed steps", t_ms, RING_SLOTS);
+  NoAllocScratch *s = nullptr;
+  rc = noalloc_scratch(e->device, &s);
+  if (rc) return rc;
+  const uint32_t slot = t_ms % RING_SLOTS;
+  const size_t off = (size_t)slot * e->hnet.N;
+  rank_select_kernel<<<1, 256, 0, e->stream>>>(e->d.ring_ids + off, e->d.ring_te + off, e->d.ring_cnt + slot,
+                                               h * e->hnet.locN, (h + 1) * e->hnet.locN, s);
+  CK(cudaGetLastError());
+  uint32_t n = 0;
+  CK(cudaMemcpyAsync(&n, &s->count, 4, cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  *count = n;
+  const uint32_t k = std::min(n, cap);
+  if (k && ids) CK(cudaMemcpyAsync(ids, s->ids, 4ull * k, cudaMemcpyDeviceToHost, e->stream));
+  if (k && te) CK(cudaMemcpyAsync(te, s->te, 8ull * k, cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
   return 0;
 }

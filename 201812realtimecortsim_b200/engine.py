@@ -53,8 +53,10 @@ EXPORTS = [
     "dpsnn_params_from_env", "dpsnn_create", "dpsnn_destroy", "dpsnn_step", "dpsnn_sync",
     "dpsnn_glob_n", "dpsnn_time_ms", "dpsnn_synapse_count", "dpsnn_events_delivered",
     "dpsnn_spikes", "dpsnn_rank_synapse_count", "dpsnn_backward_synapses", "dpsnn_state",
-    "dpsnn_bath_params", "dpsnn_set_timing", "dpsnn_kernel_times", "dpsnn_kernel_launches", "dpsnn_cuda_stream", "dpsnn_last_error",
+    "dpsnn_bath_params", "dpsnn_set_timing", "dpsnn_kernel_times", "dpsnn_kernel_launches", "dpsnn_cuda_stream",
+    "dpsnn_rank_spikes_noalloc", "dpsnn_last_error",
 ]
+NOALLOC_MAX_SPIKES = 32768   # DPSNN_NOALLOC_MAX_SPIKES
 
 _LIB = None
 
@@ -94,6 +96,8 @@ def load_library(path: str = LIB_PATH):
     lib.dpsnn_kernel_launches.restype = C.c_uint64
     lib.dpsnn_cuda_stream.argtypes = [P]
     lib.dpsnn_cuda_stream.restype = C.c_void_p
+    lib.dpsnn_rank_spikes_noalloc.argtypes = [P, C.c_uint32, C.c_uint32, P, P, C.c_uint32,
+                                              C.POINTER(C.c_uint32)]
     lib.dpsnn_last_error.restype = C.c_char_p
     _LIB = lib
     return lib
@@ -213,6 +217,18 @@ class Engine:
         if n:
             self._check(self._L.dpsnn_spikes(self._h, t_ms, _ptr(ids), _ptr(te), n, C.byref(cnt)), "dpsnn_spikes")
         return ids, te
+
+    def rank_spikes_noalloc(self, t_ms: int, rank: int):
+        """Spikes of one emulated rank at step t_ms, gathered without any
+        device allocation (dpsnn_rank_spikes_noalloc)."""
+        cnt = C.c_uint32()
+        cap = NOALLOC_MAX_SPIKES
+        ids = np.empty(cap, np.uint32)
+        te = np.empty(cap, np.float64)
+        self._check(self._L.dpsnn_rank_spikes_noalloc(self._h, t_ms, rank, _ptr(ids), _ptr(te), cap,
+                                                        C.byref(cnt)), "dpsnn_rank_spikes_noalloc")
+        n = cnt.value
+        return ids[:n].copy(), te[:n].copy()
 
     def backward_synapses(self, rank: int = 0, with_tderiv: bool = False):
         n = self._L.dpsnn_rank_synapse_count(self._h, rank)

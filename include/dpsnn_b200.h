@@ -145,6 +145,24 @@ uint64_t dpsnn_kernel_launches(const dpsnn_engine *e);
  * with CUDA events by the caller). */
 void *dpsnn_cuda_stream(const dpsnn_engine *e);
 
+/* Spike list of emulated rank h at step t_ms (one of the last 80 steps):
+ * the entries of dpsnn_spikes() whose neuron belongs to rank h, same order.
+ * No counterpart in the reference: it is the spike list one reference rank
+ * holds (spikingNeuronIdsInThisTimeStep, DPSNN_localNet_sim.c:222-226), read
+ * without any device allocation, for callers that must not allocate -- a
+ * real-time loop reading a rank's raster every 1 ms step (cudaMalloc and
+ * cudaFree synchronise the whole device and can take longer than a step) or
+ * a host that budgets every byte of device memory itself.  The gather goes
+ * through a fixed scratch area in the library image holding
+ * DPSNN_NOALLOC_MAX_SPIKES spikes (384 KiB); engines whose ranks hold more
+ * neurons get DPSNN_E_CAPACITY.  There is one scratch per device and process:
+ * calls that overlap in time on the same device (from several threads, or
+ * several engines on one device) race on it and must be serialised by the
+ * caller. */
+#define DPSNN_NOALLOC_MAX_SPIKES 32768
+int dpsnn_rank_spikes_noalloc(dpsnn_engine *e, uint32_t t_ms, uint32_t h, uint32_t *ids, double *te,
+                              uint32_t cap, uint32_t *count);
+
 const char *dpsnn_last_error(void);
 
 #ifdef __cplusplus
