@@ -536,22 +536,31 @@ __global__ void deliver_kernel(Dev d) {
 //   warp 1     extends the lagged Fibonacci sequence 24 values per round
 //              (x[n] = x[n-55] - x[n-24] mod 1e9) into a ring of raw draws;
 //   warps 2..7 convert each round into the LUT index (uint32)(u*256) and the
-//              lapse factor -logf((float)(1-u));
-//   warp 0     walks the neurons: the serial chain only counts each neuron's
-//              events (all lanes in step, parameters passed by shuffles),
-//              then the 32 lanes write a 32-neuron chunk's events in
-//              parallel, each replaying its neuron from the chain's start.
-// Ring slots are published per 24-draw round with a flag; every wait is
-// bounded and raises F_BATH_DRAWS when its limit is reached.
+//              lapse factor -logf((float)(1-u)), and extend q[], the running
+//              sum over draws of one parity of the lapses in 2^-40 units
+//              (q[n] = q[n-2] + round(lap[n] * 2^40), exact integers);
+//   warp 0     walks the neurons.  The number of events c of a neuron is the
+//              first c at which nextBath + sum of c lapses * invNuExt reaches
+//              t+1: lane L evaluates that sum for c = L+1 from two q[] reads
+//              and one ballot gives c.  Where a sum lies within a rounding
+//              bound of t+1 (or c > 32, or the maxExternCurrentCount cap is
+//              reached), the reference's sequential loop decides instead.
+//              Then the 32 lanes write a 32-neuron chunk's events in
+//              parallel, each replaying its neuron in the reference's exact
+//              arithmetic.
+// Rounds are published in order with a flag; every wait is bounded and
+// raises F_BATH_DRAWS when its limit is reached.
 #define BATH_THREADS 256
 #define BATH_RING 8192         // draws resident in shared memory
 #define BATH_ROUNDS 512        // round flags tracked (BATH_ROUNDS*24 > BATH_RING)
 #define BATH_MAX_EXT 2048      // largest maxExternCurrentCount supported
 #define BATH_SPIN_LIMIT (1u << 26)
+#define BATH_FAST_LANES 32     // events decided by one ballot
+#define BATH_WINDOW (2 * BATH_FAST_LANES + 2)   // draws a ballot reads past pos
 
 struct BathSmem {
-  float lap[BATH_RING];
-  uint32_t raw[BATH_RING];
+  uint32_t lap[BATH_RING];          // raw draw until converted, then the lapse (float bits)
+  unsigned long long q[BATH_RING];  // per-parity prefix of the lapses, 2^-40 units
   uint8_t idx[BATH_RING];
   uint32_t flag[BATH_ROUNDS];       // round r converted <=> flag[r % BATH_ROUNDS] == r + 1
   uint32_t hist[64];
@@ -559,6 +568,7 @@ struct BathSmem {
   unsigned long long raw_end;       // draws generated
   unsigned long long conv_base;     // first draw of round 0 of this launch
   uint32_t next_round;              // next round a converter claims
+  uint32_t published;               // rounds 0 .. published-1 are converted
   uint32_t done, err;
 };
 
@@ -580,14 +590,18 @@ __device__ static inline float logf_ref_dev(const logf_fixup_t &fx, const uint32
   return (lo < fx.n && __ldg(&fx.keys[lo]) == key) ? __ldg(&fx.vals[lo]) : f;
 }
 
-__device__ static inline void bath_convert(const Dev &d, BathSmem &s, unsigned long long n) {
-  const uint32_t k = (uint32_t)n & (BATH_RING - 1);
-  const uint32_t mj = s.raw[k];
+// Converts raw draw mj into (LUT index, lapse) (getPoissonLapse, :844-865,
+// and the LUT index draw at :617-619).
+__device__ static inline float bath_lapse(const Dev &d, uint32_t mj, uint8_t &idx) {
   const double u = mj * (1.0 / (double)MBIG);
-  s.idx[k] = (uint8_t)(uint32_t)(u * 256);
+  idx = (uint8_t)(uint32_t)(u * 256);
   double temp = (double)1.0 - u;
   if (temp < 0) temp = 0;
-  s.lap[k] = -logf_ref_dev(d.fix, d.fix_bitmap, (float)temp);
+  return -logf_ref_dev(d.fix, d.fix_bitmap, (float)temp);
+}
+
+__device__ static inline unsigned long long lap_fixed(float lap) {
+  return __double2ull_rn((double)lap * 0x1p40);
 }
 
 __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
@@ -596,12 +610,13 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
   volatile BathSmem &vs = s;
   const NetConst *net = d.net;
   const uint32_t h = blockIdx.x, t = *d.t, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t M = BATH_RING - 1;
   // restore: generator history, consumer position, draws converted last launch
   const unsigned long long p0 = d.bath_pos[h], q0 = d.bath_produced[h];
   if (tid < 64) s.hist[tid] = d.bath_hist[h * 64 + tid];
   for (unsigned long long n = p0 + tid; n < q0; n += blockDim.x) {
-    const uint32_t k = (uint32_t)n & (BATH_RING - 1);
-    s.lap[k] = d.draw_lapse[(size_t)h * BATH_RING + k];
+    const uint32_t k = (uint32_t)n & M;
+    s.lap[k] = __float_as_uint(d.draw_lapse[(size_t)h * BATH_RING + k]);
     s.idx[k] = d.draw_idx[(size_t)h * BATH_RING + k];
   }
   for (uint32_t r = tid; r < BATH_ROUNDS; r += blockDim.x) s.flag[r] = 0;
@@ -610,8 +625,26 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
     s.raw_end = q0;
     s.conv_base = q0;
     s.next_round = 0;
+    s.published = 0;
     s.done = 0;
     s.err = 0;
+    s.q[(p0 - 2) & M] = 0;   // the prefix starts at p0 in each launch
+    s.q[(p0 - 1) & M] = 0;
+  }
+  __syncthreads();
+  if (warp == 0) {   // prefix of the restored draws [p0, q0)
+    for (unsigned long long n0 = p0; n0 < q0; n0 += 32) {
+      const unsigned long long n = n0 + lane;
+      unsigned long long v = (n < q0) ? lap_fixed(__uint_as_float(s.lap[n & M])) : 0ull;
+      for (int o = 2; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= (uint32_t)o) v += y;
+      }
+      v += s.q[(n0 - 2 + (lane & 1)) & M];
+      __syncwarp();
+      if (n < q0) s.q[n & M] = v;
+      __syncwarp();
+    }
   }
   __syncthreads();
   const double T1 = (double)((double)t + 1.0);
@@ -637,7 +670,7 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
       __syncwarp();
       if (lane < 24) {
         s.hist[nn & 63] = (uint32_t)x;
-        s.raw[nn & (BATH_RING - 1)] = (uint32_t)x;
+        s.lap[nn & M] = (uint32_t)x;
       }
       __syncwarp();
       __threadfence_block();
@@ -645,7 +678,7 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
       r++;
     }
   } else if (warp >= 2) {
-    // ---- converters
+    // ---- converters: rounds are claimed in order and published in order
     while (true) {
       uint32_t r = 0;
       if (lane == 0) r = atomicAdd(&s.next_round, 1u);
@@ -660,10 +693,38 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
       }
       if (quit) break;
       __threadfence_block();
-      if (lane < 24) bath_convert(d, s, n0 + lane);
+      uint8_t ix = 0;
+      float lp = 0.0f;
+      if (lane < 24) lp = bath_lapse(d, vs.lap[(n0 + lane) & M], ix);
+      unsigned long long v = (lane < 24) ? lap_fixed(lp) : 0ull;
+      for (int o = 2; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= (uint32_t)o) v += y;
+      }
+      // the previous round's prefix is final once its flag is set
+      if (r > 0) {
+        spins = 0;
+        while (true) {
+          if (vs.flag[(r - 1) % BATH_ROUNDS] == r) break;
+          if (vs.done) { quit = true; break; }
+          if (++spins > BATH_SPIN_LIMIT) { vs.err = 1; vs.done = 1; quit = true; break; }
+        }
+        if (quit) break;   // nothing of this round was written
+        __threadfence_block();
+      }
+      v += vs.q[(n0 - 2 + (lane & 1)) & M];
+      if (lane < 24) {
+        const uint32_t k = (uint32_t)(n0 + lane) & M;
+        s.lap[k] = __float_as_uint(lp);
+        s.idx[k] = ix;
+        s.q[k] = v;
+      }
       __syncwarp();
       __threadfence_block();
-      if (lane == 0) vs.flag[r % BATH_ROUNDS] = r + 1;
+      if (lane == 0) {
+        vs.flag[r % BATH_ROUNDS] = r + 1;
+        vs.published = r + 1;
+      }
     }
   } else {
     // ---- consumer (warp 0)
@@ -679,6 +740,7 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
       nx_inv = d.inv_nu[i0 + lane];
       nx_mx = d.max_ext[i0 + lane];
     }
+    const double tol_base = 0x1p-30 * (fabs(T1) + 1.0);
     for (uint32_t c0 = 0; c0 < locN && !fail; c0 += 32) {
       const uint32_t cn = min(32u, locN - c0);
       const double my_nb = nx_nb, my_inv = nx_inv;
@@ -698,8 +760,9 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
         const double n_nb = __shfl_sync(0xffffffffu, my_nb, jn);
         const double n_inv = __shfl_sync(0xffffffffu, my_inv, jn);
         const uint32_t n_mx = __shfl_sync(0xffffffffu, my_mx, jn);
+        const unsigned long long need = max(2ull * mx + 4, (unsigned long long)BATH_WINDOW);
         uint32_t spins = 0;
-        while (lim < pos + 2ull * mx + 4) {
+        while (lim < pos + need) {
           if (vs.flag[rr % BATH_ROUNDS] == rr + 1) {
             rr++;
             lim = s.conv_base + (unsigned long long)rr * 24;
@@ -713,30 +776,44 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
         const unsigned long long start = pos;
         uint32_t c = 0;
         if (inv > 0 && nbv < T1) {
-          float ln = s.lap[(pos + 1) & (BATH_RING - 1)];
-          do {
-            c++;
-            const double step = (double)ln * inv;
-            pos += 2;
-            ln = s.lap[(pos + 1) & (BATH_RING - 1)];
-            nbv += step;
-          } while ((nbv < T1) && (c < mx));
-          if (c >= mx && nbv < T1) {
-            do {   // single draws past the cap (rare)
-              while (lim <= pos) {
-                if (vs.flag[rr % BATH_ROUNDS] == rr + 1) {
-                  rr++;
-                  lim = s.conv_base + (unsigned long long)rr * 24;
-                  __threadfence_block();
-                } else if (++spins > BATH_SPIN_LIMIT) {
-                  fail = true;
-                  break;
+          // lane L: nextBath + (lapses pos+1, pos+3, .., pos+1+2L) * invNuExt
+          const unsigned long long qb = s.q[(pos - 1) & M];
+          const unsigned long long qa = s.q[(pos + 1 + 2 * lane) & M];
+          const double A = nbv + inv * ((double)(qa - qb) * 0x1p-40);
+          const double tol = tol_base + inv * 0x1p-34;
+          const uint32_t below = __ballot_sync(0xffffffffu, A < T1 - tol);
+          const uint32_t above = __ballot_sync(0xffffffffu, A > T1 + tol);
+          const uint32_t m = __popc(below);
+          if (m < 32 && ((above >> m) & 1u) && below == ((1u << m) - 1u) && m + 1 <= mx) {
+            c = m + 1;
+            pos += 2ull * c;
+          } else {
+            // the reference's loop (regularDynamicTimeStep :604-640)
+            float ln = __uint_as_float(s.lap[(pos + 1) & M]);
+            do {
+              c++;
+              const double step = (double)ln * inv;
+              pos += 2;
+              ln = __uint_as_float(s.lap[(pos + 1) & M]);
+              nbv += step;
+            } while ((nbv < T1) && (c < mx));
+            if (c >= mx && nbv < T1) {
+              do {   // single draws past the cap (rare)
+                while (lim <= pos) {
+                  if (vs.flag[rr % BATH_ROUNDS] == rr + 1) {
+                    rr++;
+                    lim = s.conv_base + (unsigned long long)rr * 24;
+                    __threadfence_block();
+                  } else if (++spins > BATH_SPIN_LIMIT) {
+                    fail = true;
+                    break;
+                  }
                 }
-              }
-              if (fail) break;
-              nbv += (double)s.lap[pos & (BATH_RING - 1)] * inv;
-              pos += 1;
-            } while (nbv < T1);
+                if (fail) break;
+                nbv += (double)__uint_as_float(s.lap[pos & M]) * inv;
+                pos += 1;
+              } while (nbv < T1);
+            }
           }
         }
         if (fail) break;
@@ -764,13 +841,13 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
         uint8_t *bl = d.bath_lut + ev_base + my_off;
         for (uint32_t c = 0; c < my_cnt; c++) {
           bt[c] = v;
-          bl[c] = s.idx[p & (BATH_RING - 1)];
-          v += (double)s.lap[(p + 1) & (BATH_RING - 1)] * my_inv;
+          bl[c] = s.idx[p & M];
+          v += (double)__uint_as_float(s.lap[(p + 1) & M]) * my_inv;
           p += 2;
         }
         if (my_cnt >= my_mx && my_cnt > 0 && v < T1) {
           do {
-            v += (double)s.lap[p & (BATH_RING - 1)] * my_inv;
+            v += (double)__uint_as_float(s.lap[p & M]) * my_inv;
             p += 1;
           } while (v < T1);
         }
@@ -793,16 +870,19 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
     if (tid == 0) atomicOr(d.flags, F_BATH_DRAWS);
     return;
   }
-  // convert the generated rounds no converter reached, then save the state
+  // convert the generated rounds no converter published (they follow the
+  // published ones, and still hold raw draws), then save the state
   const unsigned long long re = s.raw_end;
-  for (unsigned long long n = s.conv_base + tid; n < re; n += blockDim.x) {
-    const uint32_t r = (uint32_t)((n - s.conv_base) / 24);
-    if (s.flag[r % BATH_ROUNDS] != r + 1) bath_convert(d, s, n);
+  for (unsigned long long n = s.conv_base + 24ull * s.published + tid; n < re; n += blockDim.x) {
+    uint8_t ix = 0;
+    const float lp = bath_lapse(d, s.lap[n & M], ix);
+    s.lap[n & M] = __float_as_uint(lp);
+    s.idx[n & M] = ix;
   }
   __syncthreads();
   for (unsigned long long n = s.pos + tid; n < re; n += blockDim.x) {
-    const uint32_t k = (uint32_t)n & (BATH_RING - 1);
-    d.draw_lapse[(size_t)h * BATH_RING + k] = s.lap[k];
+    const uint32_t k = (uint32_t)n & M;
+    d.draw_lapse[(size_t)h * BATH_RING + k] = __uint_as_float(s.lap[k]);
     d.draw_idx[(size_t)h * BATH_RING + k] = s.idx[k];
   }
   if (tid < 64) d.bath_hist[h * 64 + tid] = s.hist[tid];
@@ -1263,8 +1343,8 @@ struct dpsnn_engine {
   struct TimedLaunch { int family; cudaEvent_t a, b; };
   std::vector<TimedLaunch> pending;   // recorded, not yet read
   std::vector<cudaEvent_t> event_pool;
-  double ktime[5] = {0, 0, 0, 0, 0};
-  uint64_t klaunch[5] = {0, 0, 0, 0, 0};
+  double ktime[DPSNN_TIMING_SLOTS] = {};
+  uint64_t klaunch[DPSNN_TIMING_SLOTS] = {};
   uint64_t launches = 0;               // kernels enqueued by dpsnn_step
   std::vector<float> fix_vals;
   std::vector<uint32_t> fix_keys, fix_bucket;
@@ -1864,10 +1944,16 @@ static int enqueue_step(dpsnn_engine *e) {
   timed_launch_end(e, 2);
   timed_launch_begin(e, 3);
   neuron_kernel<<<e->grid_neuron, NEURON_BLOCK, 0, e->stream>>>(d);
-  heavy_sort_kernel<<<e->grid_heavy, HEAVY_SORT_WARPS * 32, HEAVY_SORT_SMEM, e->stream>>>(d);
-  heavy_run_kernel<<<e->grid_heavy, 128, 0, e->stream>>>(d);
-  huge_kernel<<<e->grid_heavy, HEAVY_THREADS, HEAVY_SMEM, e->stream>>>(d);
   timed_launch_end(e, 3);
+  timed_launch_begin(e, 5);
+  heavy_sort_kernel<<<e->grid_heavy, HEAVY_SORT_WARPS * 32, HEAVY_SORT_SMEM, e->stream>>>(d);
+  timed_launch_end(e, 5);
+  timed_launch_begin(e, 6);
+  heavy_run_kernel<<<e->grid_heavy, 128, 0, e->stream>>>(d);
+  timed_launch_end(e, 6);
+  timed_launch_begin(e, 7);
+  huge_kernel<<<e->grid_heavy, HEAVY_THREADS, HEAVY_SMEM, e->stream>>>(d);
+  timed_launch_end(e, 7);
   if (e->hnet.stdp_on) {
     timed_launch_begin(e, 4);
     ltp_kernel<<<e->grid_deliver, 256, 0, e->stream>>>(d);
@@ -2024,13 +2110,13 @@ extern "C" int dpsnn_set_timing(dpsnn_engine *e, int enable) {
 extern "C" uint64_t dpsnn_kernel_launches(const dpsnn_engine *e) { return e ? e->launches : 0; }
 extern "C" void *dpsnn_cuda_stream(const dpsnn_engine *e) { return e ? (void *)e->stream : nullptr; }
 
-extern "C" int dpsnn_kernel_times(dpsnn_engine *e, double *seconds5, uint64_t *launches5) {
+extern "C" int dpsnn_kernel_times(dpsnn_engine *e, double *seconds, uint64_t *launches) {
   if (!e) return dpsnn_fail(DPSNN_E_PARAM, "null engine");
   cudaSetDevice(e->device);
   collect_timings(e);
-  for (int k = 0; k < 5; k++) {
-    if (seconds5) seconds5[k] = e->ktime[k];
-    if (launches5) launches5[k] = e->klaunch[k];
+  for (int k = 0; k < DPSNN_TIMING_SLOTS; k++) {
+    if (seconds) seconds[k] = e->ktime[k];
+    if (launches) launches[k] = e->klaunch[k];
   }
   return 0;
 }

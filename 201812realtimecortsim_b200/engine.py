@@ -57,6 +57,8 @@ EXPORTS = [
     "dpsnn_rank_spikes_noalloc", "dpsnn_last_error",
 ]
 NOALLOC_MAX_SPIKES = 32768   # DPSNN_NOALLOC_MAX_SPIKES
+TIMING_SLOTS = 8             # DPSNN_TIMING_SLOTS
+TIMING_NAMES = ["compact", "deliver", "bath", "neuron", "plasticity", "heavy_sort", "heavy_run", "huge"]
 
 _LIB = None
 
@@ -263,8 +265,8 @@ class Engine:
         return self._L.dpsnn_kernel_launches(self._h)
 
     def kernel_times(self):
-        sec = np.zeros(5, np.float64)
-        cnt = np.zeros(5, np.uint64)
+        sec = np.zeros(TIMING_SLOTS, np.float64)
+        cnt = np.zeros(TIMING_SLOTS, np.uint64)
         self._check(self._L.dpsnn_kernel_times(self._h, _ptr(sec), _ptr(cnt)), "dpsnn_kernel_times")
         return sec, cnt
 

@@ -233,6 +233,7 @@ def main():
     workload = WORKLOAD if (cfx, cfy, args.ranks) == (24, 24, 192) else (
         f"{cfx}x{cfy} grid, {cfg.glob_n} neurons, 1 ms steps, STDP off, RNG streams of {args.ranks} ranks")
     eng = E.Engine(cfg, device=local)
+    eng_bytes = 6 * eng.synapse_count
     eng.step(args.warmup)
     eng.sync()
     stream = torch.cuda.ExternalStream(eng.cuda_stream())
@@ -305,10 +306,10 @@ def main():
     eng.close()
 
     hbm, peak_kind = peaks()
-    fam = ["compact", "deliver", "bath", "neuron", "plasticity"]
+    fam = E.TIMING_NAMES
     fam_total = float(sum(ksec)) or 1.0
     kernel_share = {f: float(s) / fam_total for f, s in zip(fam, ksec)}
-    kernel_ms = {f: (1e3 * float(s) / int(c) if c else 0.0) for f, s, c in zip(fam, ksec, kcnt)}
+    kernel_ms = {f: (1e3 * float(s) / prof_steps) for f, s in zip(fam, ksec)}   # per step
     # delivery kernel: per synaptic event it reads the u32 target and the
     # i16 weight of the synapse and writes one 8-byte {key, weight} record
     deliver_s = float(ksec[1]) / max(int(kcnt[1]), 1)
@@ -337,14 +338,14 @@ def main():
             "data": "synthetic: network generated by the reference's algorithm, seed 1",
             "config": {"workload": workload, "global_batch": world, "seq_len": args.steps,
                        "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (connectome ~5 GB read every step)",
+                       "l2": f"inputs larger than L2 (connectome {eng_bytes / 1e9:.1f} GB of CSR read every step)",
                        "real_time_factor": t_max / (args.steps * 1e-3),
                        "events_per_step": events / args.steps},
             "roofline": {"bound": "hbm", "kernel": "deliver_kernel", "achieved": achieved, "peak": hbm,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": traffic, "algorithmic_bytes_per_event": 14,
                          "events_per_launch": ev_per_launch},
-            "kernel_ms": kernel_ms,
+            "kernel_ms_per_step": kernel_ms,
             "kernel_share": kernel_share,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": d2h / max(e2e_steps, 1), "steps": e2e_steps,

@@ -133,12 +133,15 @@ int dpsnn_state(dpsnn_engine *e, double *v, double *c, double *tr, double *te, d
 /* Per-neuron bath parameters (invNuExt, maxExternCurrentCount). */
 int dpsnn_bath_params(dpsnn_engine *e, double *inv_nu_ext, uint32_t *max_ext);
 
-/* Seconds of device time spent in each kernel family since creation
- * (index: 0 compaction, 1 delivery, 2 bath, 3 neuron update, 4 plasticity);
- * counted only while timing is enabled with dpsnn_set_timing(e, 1), which
- * records CUDA events around each family without synchronising. */
+/* Seconds of device time spent in each kernel since creation, and the
+ * number of launches timed, in DPSNN_TIMING_SLOTS slots: 0 compaction,
+ * 1 delivery, 2 bath, 3 neuron update (neurons with few events),
+ * 4 plasticity, 5/6/7 heavy-neuron sort / update / single-block update.
+ * Counted only while timing is enabled with dpsnn_set_timing(e, 1), which
+ * records CUDA events around each launch without synchronising. */
+#define DPSNN_TIMING_SLOTS 8
 int dpsnn_set_timing(dpsnn_engine *e, int enable);
-int dpsnn_kernel_times(dpsnn_engine *e, double *seconds5, uint64_t *launches5);
+int dpsnn_kernel_times(dpsnn_engine *e, double *seconds, uint64_t *launches);
 /* Kernels enqueued by dpsnn_step since creation. */
 uint64_t dpsnn_kernel_launches(const dpsnn_engine *e);
 /* The cudaStream_t all of the engine's work is enqueued on (for timing
