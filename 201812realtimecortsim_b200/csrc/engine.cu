@@ -537,14 +537,18 @@ __global__ void deliver_kernel(Dev d) {
 //              (x[n] = x[n-55] - x[n-24] mod 1e9) into a ring of raw draws;
 //   warps 2..7 convert each round into the LUT index (uint32)(u*256) and the
 //              lapse factor -logf((float)(1-u)), and extend q[], the running
-//              sum over draws of one parity of the lapses in 2^-40 units
-//              (q[n] = q[n-2] + round(lap[n] * 2^40), exact integers);
+//              sum over draws of one parity of the lapses in 2^-20 units
+//              (q[n] = q[n-2] + round(lap[n] * 2^20), integers mod 2^32);
 //   warp 0     walks the neurons.  The number of events c of a neuron is the
 //              first c at which nextBath + sum of c lapses * invNuExt reaches
-//              t+1: lane L evaluates that sum for c = L+1 from two q[] reads
-//              and one ballot gives c.  Where a sum lies within a rounding
-//              bound of t+1 (or c > 32, or the maxExternCurrentCount cap is
-//              reached), the reference's sequential loop decides instead.
+//              t+1.  Per chunk of 32 neurons each lane turns its neuron's
+//              budget (t+1 - nextBath)/invNuExt into two integer bounds that
+//              enclose every rounding of the reference's sequential sum; on
+//              the serial chain, lane L compares the sum of the next L+1
+//              lapses (two q[] reads) with the bounds and one ballot gives c.
+//              Where a sum falls between the bounds (or c > 32, or the
+//              maxExternCurrentCount cap is reached), the reference's
+//              sequential loop decides instead.
 //              Then the 32 lanes write a 32-neuron chunk's events in
 //              parallel, each replaying its neuron in the reference's exact
 //              arithmetic.
@@ -560,7 +564,7 @@ __global__ void deliver_kernel(Dev d) {
 
 struct BathSmem {
   uint32_t lap[BATH_RING];          // raw draw until converted, then the lapse (float bits)
-  unsigned long long q[BATH_RING];  // per-parity prefix of the lapses, 2^-40 units
+  uint32_t q[BATH_RING];            // per-parity prefix of the lapses, 2^-20 units
   uint8_t idx[BATH_RING];
   uint32_t flag[BATH_ROUNDS];       // round r converted <=> flag[r % BATH_ROUNDS] == r + 1
   uint32_t hist[64];
@@ -600,8 +604,8 @@ __device__ static inline float bath_lapse(const Dev &d, uint32_t mj, uint8_t &id
   return -logf_ref_dev(d.fix, d.fix_bitmap, (float)temp);
 }
 
-__device__ static inline unsigned long long lap_fixed(float lap) {
-  return __double2ull_rn((double)lap * 0x1p40);
+__device__ static inline uint32_t lap_fixed(float lap) {
+  return __double2uint_rn((double)lap * 0x1p20);   // lap < 2^11: no overflow
 }
 
 __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
@@ -635,9 +639,9 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
   if (warp == 0) {   // prefix of the restored draws [p0, q0)
     for (unsigned long long n0 = p0; n0 < q0; n0 += 32) {
       const unsigned long long n = n0 + lane;
-      unsigned long long v = (n < q0) ? lap_fixed(__uint_as_float(s.lap[n & M])) : 0ull;
+      uint32_t v = (n < q0) ? lap_fixed(__uint_as_float(s.lap[n & M])) : 0u;
       for (int o = 2; o < 32; o <<= 1) {
-        const unsigned long long y = __shfl_up_sync(0xffffffffu, v, o);
+        const uint32_t y = __shfl_up_sync(0xffffffffu, v, o);
         if (lane >= (uint32_t)o) v += y;
       }
       v += s.q[(n0 - 2 + (lane & 1)) & M];
@@ -659,6 +663,7 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
       uint32_t spins = 0;
       while (!vs.done && n0 + 24 > vs.pos + BATH_RING - 64) {
         if (++spins > BATH_SPIN_LIMIT) { vs.err = 1; vs.done = 1; break; }
+        __nanosleep(64);   // leave the issue slots to the consumer
       }
       if (vs.done) break;
       const uint32_t nn = (uint32_t)(n0 + lane);
@@ -690,15 +695,16 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
         if (vs.raw_end >= n0 + 24) break;
         if (vs.done) { quit = true; break; }
         if (++spins > BATH_SPIN_LIMIT) { vs.err = 1; vs.done = 1; quit = true; break; }
+        __nanosleep(64);
       }
       if (quit) break;
       __threadfence_block();
       uint8_t ix = 0;
       float lp = 0.0f;
       if (lane < 24) lp = bath_lapse(d, vs.lap[(n0 + lane) & M], ix);
-      unsigned long long v = (lane < 24) ? lap_fixed(lp) : 0ull;
+      uint32_t v = (lane < 24) ? lap_fixed(lp) : 0u;
       for (int o = 2; o < 32; o <<= 1) {
-        const unsigned long long y = __shfl_up_sync(0xffffffffu, v, o);
+        const uint32_t y = __shfl_up_sync(0xffffffffu, v, o);
         if (lane >= (uint32_t)o) v += y;
       }
       // the previous round's prefix is final once its flag is set
@@ -708,6 +714,7 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
           if (vs.flag[(r - 1) % BATH_ROUNDS] == r) break;
           if (vs.done) { quit = true; break; }
           if (++spins > BATH_SPIN_LIMIT) { vs.err = 1; vs.done = 1; quit = true; break; }
+          __nanosleep(32);
         }
         if (quit) break;   // nothing of this round was written
         __threadfence_block();
@@ -740,11 +747,30 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
       nx_inv = d.inv_nu[i0 + lane];
       nx_mx = d.max_ext[i0 + lane];
     }
-    const double tol_base = 0x1p-30 * (fabs(T1) + 1.0);
     for (uint32_t c0 = 0; c0 < locN && !fail; c0 += 32) {
       const uint32_t cn = min(32u, locN - c0);
       const double my_nb = nx_nb, my_inv = nx_inv;
       const uint32_t my_mx = nx_mx;
+      // Integer bounds on the lapse sum, in 2^-20 units, for this lane's
+      // neuron: a fixed-point sum F of c lapses below my_lo means the
+      // reference's sequential nextBath after c events is certainly < t+1,
+      // above my_hi certainly >= t+1.  E1 bounds the rounding of that
+      // sequential sum (c <= 32 additions, |values| < |T1| + 42 invNuExt,
+      // and t+1 - nextBath); 2^-16 bounds the rounding of F (32 terms of at
+      // most 2^-21); the 2^-30 relative margin covers the bound's own
+      // arithmetic.
+      const int my_act = (my_inv > 0 && my_nb < T1) ? 1 : 0;
+      long long my_lo = 0, my_hi = 0;
+      if (my_act) {
+        const double E1 = 0x1p-44 * (fabs(T1) + fabs(my_nb) + 1.0 + 32.0 * my_inv);
+        double blo = ((T1 - my_nb) - E1) / my_inv - 0x1p-16;
+        double bhi = ((T1 - my_nb) + E1) / my_inv + 0x1p-16;
+        const double mg = 0x1p-30 * (fabs(bhi) + 1.0);
+        blo = fmin(fmax((blo - mg) * 0x1p20, -0x1p60), 0x1p60);
+        bhi = fmin(fmax((bhi + mg) * 0x1p20, -0x1p60), 0x1p60);
+        my_lo = (long long)floor(blo);
+        my_hi = (long long)ceil(bhi);
+      }
       if (c0 + 32 < locN && lane < min(32u, locN - c0 - 32)) {   // prefetch the next chunk
         nx_nb = d.nb[i0 + c0 + 32 + lane];
         nx_inv = d.inv_nu[i0 + c0 + 32 + lane];
@@ -760,6 +786,9 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
         const double n_nb = __shfl_sync(0xffffffffu, my_nb, jn);
         const double n_inv = __shfl_sync(0xffffffffu, my_inv, jn);
         const uint32_t n_mx = __shfl_sync(0xffffffffu, my_mx, jn);
+        const long long lo = __shfl_sync(0xffffffffu, my_lo, j);
+        const long long hi = __shfl_sync(0xffffffffu, my_hi, j);
+        const int act = __shfl_sync(0xffffffffu, my_act, j);
         const unsigned long long need = max(2ull * mx + 4, (unsigned long long)BATH_WINDOW);
         uint32_t spins = 0;
         while (lim < pos + need) {
@@ -775,14 +804,13 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
         if (fail) break;
         const unsigned long long start = pos;
         uint32_t c = 0;
-        if (inv > 0 && nbv < T1) {
-          // lane L: nextBath + (lapses pos+1, pos+3, .., pos+1+2L) * invNuExt
-          const unsigned long long qb = s.q[(pos - 1) & M];
-          const unsigned long long qa = s.q[(pos + 1 + 2 * lane) & M];
-          const double A = nbv + inv * ((double)(qa - qb) * 0x1p-40);
-          const double tol = tol_base + inv * 0x1p-34;
-          const uint32_t below = __ballot_sync(0xffffffffu, A < T1 - tol);
-          const uint32_t above = __ballot_sync(0xffffffffu, A > T1 + tol);
+        if (act) {
+          // lane L: the lapses at pos+1, pos+3, .., pos+1+2L, in 2^-20 units
+          const uint32_t qb = s.q[(pos - 1) & M];
+          const uint32_t qa = s.q[(pos + 1 + 2 * lane) & M];
+          const long long F = (long long)(uint32_t)(qa - qb);
+          const uint32_t below = __ballot_sync(0xffffffffu, F < lo);
+          const uint32_t above = __ballot_sync(0xffffffffu, F > hi);
           const uint32_t m = __popc(below);
           if (m < 32 && ((above >> m) & 1u) && below == ((1u << m) - 1u) && m + 1 <= mx) {
             c = m + 1;
@@ -1024,12 +1052,13 @@ __global__ void __launch_bounds__(NEURON_BLOCK) neuron_kernel(Dev d) {
 }
 
 // Heavy neurons, more than LOCAL_EVENTS synaptic events in one step.
-// heavy_sort_kernel: one warp per neuron loads its bucket into shared memory,
-// computes the arrival times, bitonic-sorts by (time, key) and writes the
-// sorted events back into the bucket; heavy_run_kernel then runs the neurons
-// one thread each.  Neurons with more events than the bucket holds (the rest
-// sit in the overflow list) are sorted and run by huge_kernel, one block each.
-#define HEAVY_WARP_MAX 1024
+// heavy_sort_kernel: one warp per neuron with at most HEAVY_WARP_MAX events
+// loads its bucket into shared memory, computes the arrival times,
+// bitonic-sorts by (time, key) and writes the sorted events back into the
+// bucket; heavy_run_kernel then runs those neurons one thread each.  Neurons
+// with more events (including any beyond the bucket, in the overflow list)
+// are sorted and run by huge_kernel, one block each.
+#define HEAVY_WARP_MAX 256     // events a warp sorts in shared memory
 #define HEAVY_SORT_WARPS 4
 #define HEAVY_SORT_SMEM (HEAVY_SORT_WARPS * HEAVY_WARP_MAX * 16)
 #define HEAVY_MAX 8192
@@ -1338,7 +1367,7 @@ struct dpsnn_engine {
   uint64_t S = 0;
   uint32_t t_host = 0;   // steps enqueued
   std::vector<void *> allocs;
-  uint32_t grid_neuron = 0, grid_deliver = 0, grid_heavy = 0;
+  uint32_t grid_neuron = 0, grid_deliver = 0, grid_heavy = 0, grid_heavy_run = 0, grid_huge = 0;
   int timing = 0;
   struct TimedLaunch { int family; cudaEvent_t a, b; };
   std::vector<TimedLaunch> pending;   // recorded, not yet read
@@ -1829,7 +1858,9 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
   e->grid_deliver = (uint32_t)sms * 8;
-  e->grid_heavy = (uint32_t)sms * 4;
+  e->grid_heavy = (uint32_t)sms * 14;      // 16 KB of shared memory per block
+  e->grid_heavy_run = (uint32_t)sms * 16;
+  e->grid_huge = (uint32_t)sms;
   CK(cudaFuncSetAttribute(bath_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(BathSmem)));
   CK(cudaFuncSetAttribute(huge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, HEAVY_SMEM));
   CK(cudaFuncSetAttribute(heavy_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, HEAVY_SORT_SMEM));
@@ -1949,10 +1980,10 @@ static int enqueue_step(dpsnn_engine *e) {
   heavy_sort_kernel<<<e->grid_heavy, HEAVY_SORT_WARPS * 32, HEAVY_SORT_SMEM, e->stream>>>(d);
   timed_launch_end(e, 5);
   timed_launch_begin(e, 6);
-  heavy_run_kernel<<<e->grid_heavy, 128, 0, e->stream>>>(d);
+  heavy_run_kernel<<<e->grid_heavy_run, 128, 0, e->stream>>>(d);
   timed_launch_end(e, 6);
   timed_launch_begin(e, 7);
-  huge_kernel<<<e->grid_heavy, HEAVY_THREADS, HEAVY_SMEM, e->stream>>>(d);
+  huge_kernel<<<e->grid_huge, HEAVY_THREADS, HEAVY_SMEM, e->stream>>>(d);
   timed_launch_end(e, 7);
   if (e->hnet.stdp_on) {
     timed_launch_begin(e, 4);
