@@ -360,6 +360,7 @@ struct Dev {
   double *lut;              // [nsub*256]
   // neurons
   double *v, *c, *tr, *te, *nb, *inv_nu;
+  const double *nb_prev;    // nextBath before this step's bath (bath_kernel input)
   uint32_t *max_ext;
   uint8_t *sub, *fired;
   int32_t *last_spike_ms;
@@ -469,15 +470,44 @@ __global__ void causal_stdp_kernel(Dev d) {
 
 // Step 2: delivery (axonalSpikeSchedulersToSynapticSpikeSchedulers,
 // DPSNN_localNet_sim.c:837-999, and findAndGetNextSyn, DPSNN_synapse.c:179-267).
-// Work item = (delay d, spike q of the slot written d steps ago); one warp
-// walks the CSR segment (pre, d) and appends {key, weight} to each target's
-// event list.  key = (D-1-d) << 25 | q orders a target's events as the
-// reference delivers them (delay descending, then source ascending), which
-// breaks ties between equal arrival times.
-__global__ void deliver_kernel(Dev d) {
+// Work item = (delay d, spike q of the slot written d steps ago), i.e. the CSR
+// segment (pre, d).  A warp takes 32 work items at a time: each lane fetches
+// one item's segment bounds, then the warp walks the concatenation of the 32
+// segments with every lane on a different synapse, DELIVER_UNROLL synapses
+// per lane in flight, appending {key, weight} to each target's event list.
+// key = (D-1-d) << 25 | q orders a target's events as the reference delivers
+// them (delay descending, then source ascending), which breaks ties between
+// equal arrival times.
+#define DELIVER_THREADS 256
+#define DELIVER_UNROLL 4
+
+__device__ static inline void deliver_event(const Dev &d, const NetConst *net, uint64_t k, uint32_t key,
+                                            uint32_t t, bool stdp, uint32_t cap, uint32_t j, float wf) {
+  const uint32_t s = atomicAdd(&d.ev_cnt[j], 1u);
+  if (s < cap) {
+    d.ev[(size_t)j * cap + s] = make_uint2(key, __float_as_uint(wf));
+  } else {
+    const uint32_t o = atomicAdd(d.ovf_cnt, 1u);
+    if (o < net->ovf_cap)
+      d.ovf[o] = make_uint4(j, key, __float_as_uint(wf), 0u);
+    else
+      atomicOr(d.flags, F_OVERFLOW);
+  }
+  if (stdp) {  // synapseSetLastActiveTime_antiCausalSTDP (DPSNN_neuron_sim.c:179-277)
+    d.last_act[k] = (int32_t)t;
+    const int td = (int)t - d.last_spike_ms[j];
+    const float a = (td < 128) ? net->anti_tab[td] : 0.0f;
+    d.tderiv[k] = d.tderiv[k] + a;
+  }
+}
+
+__global__ void __launch_bounds__(DELIVER_THREADS) deliver_kernel(Dev d) {
   const NetConst *net = d.net;
   const uint32_t t = *d.t, N = net->N, D = net->D, cap = net->ev_cap;
   __shared__ uint32_t s_pre[RING_SLOTS + 1];
+  __shared__ uint32_t s_off[DELIVER_THREADS / 32][33];     // per warp: exclusive prefix of lengths
+  __shared__ unsigned long long s_beg[DELIVER_THREADS / 32][32];
+  __shared__ uint32_t s_key[DELIVER_THREADS / 32][32];
   if (threadIdx.x == 0) {
     uint32_t acc = 0;
     for (uint32_t dd = 0; dd < D; dd++) {
@@ -488,43 +518,68 @@ __global__ void deliver_kernel(Dev d) {
   }
   __syncthreads();
   const uint32_t total = s_pre[D];
-  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
   const bool stdp = net->stdp_on && t >= net->start_pl && t <= net->stop_pl;
   const float w2f = net->w2f;
+  uint32_t *off = s_off[wb];
+  unsigned long long *bg = s_beg[wb];
+  uint32_t *ky = s_key[wb];
   unsigned long long my_events = 0;
-  for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < total;
-       w += (gridDim.x * blockDim.x) >> 5) {
-    uint32_t dl = 0;
-    while (s_pre[dl + 1] <= w) dl++;
-    uint32_t q = w - s_pre[dl];
-    uint32_t slot = (t + RING_SLOTS - dl) % RING_SLOTS;
-    uint32_t P = d.ring_ids[(size_t)slot * N + q];
-    uint64_t base = d.row_ptr[P];
-    const uint16_t *so = d.sub_off + (size_t)P * (D + 1);
-    uint64_t beg = base + so[dl], end = base + so[dl + 1];
-    uint32_t key = ((D - 1 - dl) << 25) | q;
-    my_events += end - beg;
-    for (uint64_t k = beg + lane; k < end; k += 32) {
-      uint32_t j = d.post[k];
-      float wf = ((float)d.w16[k]) * w2f;
-      uint32_t s = atomicAdd(&d.ev_cnt[j], 1u);
-      if (s < cap) {
-        d.ev[(size_t)j * cap + s] = make_uint2(key, __float_as_uint(wf));
-      } else {
-        uint32_t o = atomicAdd(d.ovf_cnt, 1u);
-        if (o < net->ovf_cap)
-          d.ovf[o] = make_uint4(j, key, __float_as_uint(wf), 0u);
-        else
-          atomicOr(d.flags, F_OVERFLOW);
-      }
-      if (stdp) {  // synapseSetLastActiveTime_antiCausalSTDP (DPSNN_neuron_sim.c:179-277)
-        d.last_act[k] = (int32_t)t;
-        int td = (int)t - d.last_spike_ms[j];
-        float a = (td < 128) ? net->anti_tab[td] : 0.0f;
-        d.tderiv[k] = d.tderiv[k] + a;
-      }
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t w0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u; w0 < total; w0 += nwarps * 32u) {
+    const uint32_t w = w0 + lane;
+    uint64_t beg = 0;
+    uint32_t len = 0, key = 0;
+    if (w < total) {
+      uint32_t dl = 0;
+      while (s_pre[dl + 1] <= w) dl++;
+      const uint32_t q = w - s_pre[dl];
+      const uint32_t slot = (t + RING_SLOTS - dl) % RING_SLOTS;
+      const uint32_t P = d.ring_ids[(size_t)slot * N + q];
+      const uint16_t *so = d.sub_off + (size_t)P * (D + 1);
+      const uint32_t a = so[dl], b = so[dl + 1];
+      beg = d.row_ptr[P] + a;
+      len = b - a;
+      key = ((D - 1 - dl) << 25) | q;
     }
+    uint32_t incl = len;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= (uint32_t)o) incl += y;
+    }
+    const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
+    __syncwarp();
+    off[lane] = incl - len;
+    if (lane == 31) off[32] = tot;
+    bg[lane] = beg;
+    ky[lane] = key;
+    my_events += len;
+    __syncwarp();
+    // the concatenated segments, element e = lane + 32 * i
+    uint32_t sg = 0;
+    for (uint32_t e0 = 0; e0 < tot; e0 += 32u * DELIVER_UNROLL) {
+      uint64_t k[DELIVER_UNROLL];
+      uint32_t kk[DELIVER_UNROLL], jj[DELIVER_UNROLL];
+      float wf[DELIVER_UNROLL];
+#pragma unroll
+      for (int u = 0; u < DELIVER_UNROLL; u++) {
+        const uint32_t e = e0 + 32u * u + lane;
+        kk[u] = 0xFFFFFFFFu;
+        if (e < tot) {
+          while (off[sg + 1] <= e) sg++;
+          k[u] = bg[sg] + (e - off[sg]);
+          kk[u] = ky[sg];
+          jj[u] = __ldg(&d.post[k[u]]);
+          wf[u] = ((float)__ldg(&d.w16[k[u]])) * w2f;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < DELIVER_UNROLL; u++)
+        if (kk[u] != 0xFFFFFFFFu) deliver_event(d, net, k[u], kk[u], t, stdp, cap, jj[u], wf[u]);
+    }
+    __syncwarp();
   }
+  for (int o = 16; o > 0; o >>= 1) my_events += __shfl_down_sync(0xffffffffu, my_events, o);
   if (lane == 0 && my_events) atomicAdd(d.events, my_events);
 }
 
@@ -608,12 +663,12 @@ __device__ static inline uint32_t lap_fixed(float lap) {
   return __double2uint_rn((double)lap * 0x1p20);   // lap < 2^11: no overflow
 }
 
-__global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
+__global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d, uint32_t t) {
   extern __shared__ __align__(16) unsigned char bath_smem_raw[];
   BathSmem &s = *reinterpret_cast<BathSmem *>(bath_smem_raw);
   volatile BathSmem &vs = s;
   const NetConst *net = d.net;
-  const uint32_t h = blockIdx.x, t = *d.t, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t h = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t M = BATH_RING - 1;
   // restore: generator history, consumer position, draws converted last launch
   const unsigned long long p0 = d.bath_pos[h], q0 = d.bath_produced[h];
@@ -743,7 +798,7 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
     double nx_nb = 0, nx_inv = 0;
     uint32_t nx_mx = 0;
     if (lane < min(32u, locN)) {
-      nx_nb = d.nb[i0 + lane];
+      nx_nb = d.nb_prev[i0 + lane];
       nx_inv = d.inv_nu[i0 + lane];
       nx_mx = d.max_ext[i0 + lane];
     }
@@ -772,7 +827,7 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
         my_hi = (long long)ceil(bhi);
       }
       if (c0 + 32 < locN && lane < min(32u, locN - c0 - 32)) {   // prefetch the next chunk
-        nx_nb = d.nb[i0 + c0 + 32 + lane];
+        nx_nb = d.nb_prev[i0 + c0 + 32 + lane];
         nx_inv = d.inv_nu[i0 + c0 + 32 + lane];
         nx_mx = d.max_ext[i0 + c0 + 32 + lane];
       }
@@ -1363,13 +1418,22 @@ struct dpsnn_engine {
   NetConst hnet;
   Dev d;
   cudaStream_t stream = nullptr;
+  // The bath of step t+1 runs on bath_stream while step t runs on stream:
+  // its outputs and nextBath are double-buffered by step parity.
+  cudaStream_t bath_stream = nullptr;
+  cudaEvent_t ev_bath[2] = {nullptr, nullptr}, ev_neuron[2] = {nullptr, nullptr}, ev_start = nullptr;
+  bool bath_primed = false;
+  double *nb2[2] = {nullptr, nullptr}, *bath_time2[2] = {nullptr, nullptr};
+  uint8_t *bath_lut2[2] = {nullptr, nullptr};
+  uint32_t *bath_off2[2] = {nullptr, nullptr};
+  uint16_t *bath_cnt2[2] = {nullptr, nullptr};
   int device = 0;
   uint64_t S = 0;
   uint32_t t_host = 0;   // steps enqueued
   std::vector<void *> allocs;
   uint32_t grid_neuron = 0, grid_deliver = 0, grid_heavy = 0, grid_heavy_run = 0, grid_huge = 0;
   int timing = 0;
-  struct TimedLaunch { int family; cudaEvent_t a, b; };
+  struct TimedLaunch { int family; cudaEvent_t a, b; cudaStream_t st; };
   std::vector<TimedLaunch> pending;   // recorded, not yet read
   std::vector<cudaEvent_t> event_pool;
   double ktime[DPSNN_TIMING_SLOTS] = {};
@@ -1615,7 +1679,10 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
     CK(cudaStreamSynchronize(e->stream));
   }
   // neuron arrays
-  DALLOC(d.v, N); DALLOC(d.c, N); DALLOC(d.tr, N); DALLOC(d.te, N); DALLOC(d.nb, N);
+  DALLOC(d.v, N); DALLOC(d.c, N); DALLOC(d.tr, N); DALLOC(d.te, N);
+  DALLOC(e->nb2[0], N); DALLOC(e->nb2[1], N);
+  d.nb = e->nb2[0];
+  d.nb_prev = e->nb2[1];
   DALLOC(d.inv_nu, N); DALLOC(d.max_ext, N); DALLOC(d.sub, N); DALLOC(d.fired, N);
   DALLOC(d.last_spike_ms, N);
   e->grid_neuron = (N + NEURON_BLOCK - 1) / NEURON_BLOCK;
@@ -1803,10 +1870,16 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
     CK(cudaMemcpyAsync(d.net, &n, sizeof n, cudaMemcpyHostToDevice, e->stream));
     DALLOC(d.bath_rank_base, P + 1);
     CK(cudaMemcpyAsync(d.bath_rank_base, base.data(), 8ull * (P + 1), cudaMemcpyHostToDevice, e->stream));
-    DALLOC(d.bath_time, base[P]);
-    DALLOC(d.bath_lut, base[P]);
-    DALLOC(d.bath_off, N);
-    DALLOC(d.bath_cnt, N);
+    for (int b = 0; b < 2; b++) {
+      DALLOC(e->bath_time2[b], base[P]);
+      DALLOC(e->bath_lut2[b], base[P]);
+      DALLOC(e->bath_off2[b], N);
+      DALLOC(e->bath_cnt2[b], N);
+    }
+    d.bath_time = e->bath_time2[0];
+    d.bath_lut = e->bath_lut2[0];
+    d.bath_off = e->bath_off2[0];
+    d.bath_cnt = e->bath_cnt2[0];
     // dynamics streams: SetRandomSeed(loc_h) (DPSNN_localNet_init.c:283).
     // Rank 0 continues its generation stream; others re-initialise.
     std::vector<uint32_t> hist((size_t)P * 64, 0);
@@ -1880,9 +1953,17 @@ extern "C" int dpsnn_create(const dpsnn_params *p, const dpsnn_options *opts, dp
   } else {
     cudaGetDevice(&e->device);
   }
-  if (cudaSetDevice(e->device) != cudaSuccess || cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
-    delete e;
-    return dpsnn_fail(DPSNN_E_CUDA, "cannot set up device %d", e->device);
+  bool ok = cudaSetDevice(e->device) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&e->bath_stream, cudaStreamNonBlocking) == cudaSuccess;
+  for (int b = 0; b < 2 && ok; b++)
+    ok = cudaEventCreateWithFlags(&e->ev_bath[b], cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&e->ev_neuron[b], cudaEventDisableTiming) == cudaSuccess;
+  ok = ok && cudaEventCreateWithFlags(&e->ev_start, cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    const int dev = e->device;
+    dpsnn_destroy(e);
+    return dpsnn_fail(DPSNN_E_CUDA, "cannot set up device %d", dev);
   }
   int rc = engine_build(e, p, opts);
   if (rc) {
@@ -1897,9 +1978,16 @@ extern "C" void dpsnn_destroy(dpsnn_engine *e) {
   if (!e) return;
   cudaSetDevice(e->device);
   if (e->stream) cudaStreamSynchronize(e->stream);
+  if (e->bath_stream) cudaStreamSynchronize(e->bath_stream);
   for (void *q : e->allocs) cudaFree(q);
   collect_timings(e);
   for (cudaEvent_t ev : e->event_pool) cudaEventDestroy(ev);
+  for (int b = 0; b < 2; b++) {
+    if (e->ev_bath[b]) cudaEventDestroy(e->ev_bath[b]);
+    if (e->ev_neuron[b]) cudaEventDestroy(e->ev_neuron[b]);
+  }
+  if (e->ev_start) cudaEventDestroy(e->ev_start);
+  if (e->bath_stream) cudaStreamDestroy(e->bath_stream);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
 }
@@ -1930,19 +2018,20 @@ static cudaEvent_t pool_event(dpsnn_engine *e) {
   e->event_pool.pop_back();
   return ev;
 }
-static void timed_launch_begin(dpsnn_engine *e, int k) {
+static void timed_launch_begin(dpsnn_engine *e, int k, cudaStream_t st = nullptr) {
   if (!e->timing) return;
   dpsnn_engine::TimedLaunch tl;
   tl.family = k;
   tl.a = pool_event(e);
   tl.b = pool_event(e);
-  cudaEventRecord(tl.a, e->stream);
+  tl.st = st ? st : e->stream;
+  cudaEventRecord(tl.a, tl.st);
   e->pending.push_back(tl);
 }
 static void timed_launch_end(dpsnn_engine *e, int k) {
   if (!e->timing) return;
   (void)k;
-  cudaEventRecord(e->pending.back().b, e->stream);
+  cudaEventRecord(e->pending.back().b, e->pending.back().st);
 }
 static void collect_timings(dpsnn_engine *e) {
   for (auto &tl : e->pending) {
@@ -1957,8 +2046,43 @@ static void collect_timings(dpsnn_engine *e) {
   e->pending.clear();
 }
 
+// The bath of step t (bath_kernel) depends only on the ranks' RNG streams
+// and nextBath, not on synaptic input, so it runs one step ahead on its own
+// stream, overlapping the delivery and neuron update of the previous step.
+// Its outputs (per-neuron bath events) and nextBath live in two buffers by
+// step parity: bath(t) writes set t&1 once neuron(t-2), the last reader of
+// that set, is done; neuron(t) reads set t&1 once bath(t) is done.
+static void enqueue_bath(dpsnn_engine *e, uint32_t t) {
+  Dev db = e->d;
+  const int b = t & 1;
+  db.nb_prev = e->nb2[b ^ 1];
+  db.nb = e->nb2[b];
+  db.bath_time = e->bath_time2[b];
+  db.bath_lut = e->bath_lut2[b];
+  db.bath_off = e->bath_off2[b];
+  db.bath_cnt = e->bath_cnt2[b];
+  cudaStreamWaitEvent(e->bath_stream, e->ev_neuron[b], 0);
+  timed_launch_begin(e, 2, e->bath_stream);
+  bath_kernel<<<e->hnet.P, BATH_THREADS, sizeof(BathSmem), e->bath_stream>>>(db, t);
+  timed_launch_end(e, 2);
+  cudaEventRecord(e->ev_bath[b], e->bath_stream);
+}
+
 static int enqueue_step(dpsnn_engine *e) {
-  Dev &d = e->d;
+  const uint32_t t = e->t_host;
+  const int b = t & 1;
+  if (!e->bath_primed) {   // the first bath waits for the network build
+    cudaEventRecord(e->ev_start, e->stream);
+    cudaStreamWaitEvent(e->bath_stream, e->ev_start, 0);
+    enqueue_bath(e, t);
+    e->bath_primed = true;
+  }
+  enqueue_bath(e, t + 1);
+  Dev d = e->d;
+  d.bath_time = e->bath_time2[b];
+  d.bath_lut = e->bath_lut2[b];
+  d.bath_off = e->bath_off2[b];
+  d.bath_cnt = e->bath_cnt2[b];
   timed_launch_begin(e, 0);
   compact_kernel<<<e->grid_neuron, NEURON_BLOCK, 0, e->stream>>>(d);
   timed_launch_end(e, 0);
@@ -1968,11 +2092,9 @@ static int enqueue_step(dpsnn_engine *e) {
     timed_launch_end(e, 4);
   }
   timed_launch_begin(e, 1);
-  deliver_kernel<<<e->grid_deliver, 256, 0, e->stream>>>(d);
+  deliver_kernel<<<e->grid_deliver, DELIVER_THREADS, 0, e->stream>>>(d);
   timed_launch_end(e, 1);
-  timed_launch_begin(e, 2);
-  bath_kernel<<<e->hnet.P, BATH_THREADS, sizeof(BathSmem), e->stream>>>(d);
-  timed_launch_end(e, 2);
+  cudaStreamWaitEvent(e->stream, e->ev_bath[b], 0);
   timed_launch_begin(e, 3);
   neuron_kernel<<<e->grid_neuron, NEURON_BLOCK, 0, e->stream>>>(d);
   timed_launch_end(e, 3);
@@ -1985,6 +2107,7 @@ static int enqueue_step(dpsnn_engine *e) {
   timed_launch_begin(e, 7);
   huge_kernel<<<e->grid_huge, HEAVY_THREADS, HEAVY_SMEM, e->stream>>>(d);
   timed_launch_end(e, 7);
+  cudaEventRecord(e->ev_neuron[b], e->stream);
   if (e->hnet.stdp_on) {
     timed_launch_begin(e, 4);
     ltp_kernel<<<e->grid_deliver, 256, 0, e->stream>>>(d);
@@ -2052,7 +2175,9 @@ extern "C" int dpsnn_state(dpsnn_engine *e, double *v, double *c, double *tr, do
   if (c) CK(cudaMemcpy(c, e->d.c, B, cudaMemcpyDeviceToHost));
   if (tr) CK(cudaMemcpy(tr, e->d.tr, B, cudaMemcpyDeviceToHost));
   if (te) CK(cudaMemcpy(te, e->d.te, B, cudaMemcpyDeviceToHost));
-  if (nb) CK(cudaMemcpy(nb, e->d.nb, B, cudaMemcpyDeviceToHost));
+  // nextBath after the last completed step (the bath of the next step may
+  // already have run into the other buffer)
+  if (nb) CK(cudaMemcpy(nb, e->nb2[e->t_host ? (e->t_host - 1) & 1 : 1], B, cudaMemcpyDeviceToHost));
   return 0;
 }
 
