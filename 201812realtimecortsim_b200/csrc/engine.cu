@@ -814,17 +814,20 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d, uint32_t t) {
       // and t+1 - nextBath); 2^-16 bounds the rounding of F (32 terms of at
       // most 2^-21); the 2^-30 relative margin covers the bound's own
       // arithmetic.
-      const int my_act = (my_inv > 0 && my_nb < T1) ? 1 : 0;
-      long long my_lo = 0, my_hi = 0;
-      if (my_act) {
+      // my_lo / my_hi1: F < my_lo means certainly below, F >= my_hi1
+      // certainly reached, both clamped to 32 bits (F < 2^30).  my_misc:
+      // 0 = no bath event this step; else 0x100 | min(32, maxExternCurrentCount).
+      uint32_t my_lo = 0, my_hi1 = 0, my_misc = 0;
+      if (my_inv > 0 && my_nb < T1) {
         const double E1 = 0x1p-44 * (fabs(T1) + fabs(my_nb) + 1.0 + 32.0 * my_inv);
         double blo = ((T1 - my_nb) - E1) / my_inv - 0x1p-16;
         double bhi = ((T1 - my_nb) + E1) / my_inv + 0x1p-16;
         const double mg = 0x1p-30 * (fabs(bhi) + 1.0);
-        blo = fmin(fmax((blo - mg) * 0x1p20, -0x1p60), 0x1p60);
-        bhi = fmin(fmax((bhi + mg) * 0x1p20, -0x1p60), 0x1p60);
-        my_lo = (long long)floor(blo);
-        my_hi = (long long)ceil(bhi);
+        blo = fmin(fmax(floor((blo - mg) * 0x1p20), 0.0), 4294967295.0);
+        bhi = fmin(fmax(ceil((bhi + mg) * 0x1p20) + 1.0, 0.0), 4294967295.0);
+        my_lo = (uint32_t)blo;
+        my_hi1 = (uint32_t)bhi;
+        my_misc = 0x100u | min(32u, my_mx);
       }
       if (c0 + 32 < locN && lane < min(32u, locN - c0 - 32)) {   // prefetch the next chunk
         nx_nb = d.nb_prev[i0 + c0 + 32 + lane];
@@ -833,20 +836,12 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d, uint32_t t) {
       }
       unsigned long long my_start = 0;
       uint32_t my_cnt = 0;
-      double nbv = __shfl_sync(0xffffffffu, my_nb, 0);
-      double inv = __shfl_sync(0xffffffffu, my_inv, 0);
-      uint32_t mx = __shfl_sync(0xffffffffu, my_mx, 0);
       for (uint32_t j = 0; j < cn; j++) {
-        const uint32_t jn = (j + 1 < cn) ? j + 1 : j;
-        const double n_nb = __shfl_sync(0xffffffffu, my_nb, jn);
-        const double n_inv = __shfl_sync(0xffffffffu, my_inv, jn);
-        const uint32_t n_mx = __shfl_sync(0xffffffffu, my_mx, jn);
-        const long long lo = __shfl_sync(0xffffffffu, my_lo, j);
-        const long long hi = __shfl_sync(0xffffffffu, my_hi, j);
-        const int act = __shfl_sync(0xffffffffu, my_act, j);
-        const unsigned long long need = max(2ull * mx + 4, (unsigned long long)BATH_WINDOW);
+        const uint32_t lo = __shfl_sync(0xffffffffu, my_lo, j);
+        const uint32_t hi1 = __shfl_sync(0xffffffffu, my_hi1, j);
+        const uint32_t misc = __shfl_sync(0xffffffffu, my_misc, j);
         uint32_t spins = 0;
-        while (lim < pos + need) {
+        while (lim < pos + BATH_WINDOW) {
           if (vs.flag[rr % BATH_ROUNDS] == rr + 1) {
             rr++;
             lim = s.conv_base + (unsigned long long)rr * 24;
@@ -859,19 +854,32 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d, uint32_t t) {
         if (fail) break;
         const unsigned long long start = pos;
         uint32_t c = 0;
-        if (act) {
+        if (misc) {
           // lane L: the lapses at pos+1, pos+3, .., pos+1+2L, in 2^-20 units
-          const uint32_t qb = s.q[(pos - 1) & M];
-          const uint32_t qa = s.q[(pos + 1 + 2 * lane) & M];
-          const long long F = (long long)(uint32_t)(qa - qb);
+          const uint32_t p32 = (uint32_t)pos;
+          const uint32_t F = s.q[(p32 + 1 + 2 * lane) & M] - s.q[(p32 - 1) & M];
           const uint32_t below = __ballot_sync(0xffffffffu, F < lo);
-          const uint32_t above = __ballot_sync(0xffffffffu, F > hi);
-          const uint32_t m = __popc(below);
-          if (m < 32 && ((above >> m) & 1u) && below == ((1u << m) - 1u) && m + 1 <= mx) {
+          const uint32_t above = __ballot_sync(0xffffffffu, F >= hi1);
+          const uint32_t m = __popc(below);   // F grows with L: below is a prefix
+          if (m < (misc & 0xFFu) && ((above >> m) & 1u)) {
             c = m + 1;
             pos += 2ull * c;
           } else {
             // the reference's loop (regularDynamicTimeStep :604-640)
+            double nbv = __shfl_sync(0xffffffffu, my_nb, j);
+            const double inv = __shfl_sync(0xffffffffu, my_inv, j);
+            const uint32_t mx = __shfl_sync(0xffffffffu, my_mx, j);
+            while (lim < pos + 2ull * mx + 4) {
+              if (vs.flag[rr % BATH_ROUNDS] == rr + 1) {
+                rr++;
+                lim = s.conv_base + (unsigned long long)rr * 24;
+                __threadfence_block();
+              } else if (++spins > BATH_SPIN_LIMIT) {
+                fail = true;
+                break;
+              }
+            }
+            if (fail) break;
             float ln = __uint_as_float(s.lap[(pos + 1) & M]);
             do {
               c++;
@@ -904,9 +912,6 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d, uint32_t t) {
           my_start = start;
           my_cnt = c;
         }
-        nbv = n_nb;
-        inv = n_inv;
-        mx = n_mx;
       }
       if (fail) break;
       // parallel emission of the chunk's events
