@@ -39,6 +39,7 @@
 #define MSEED 161803398
 #define NEURON_BLOCK 256
 #define LOCAL_EVENTS 32        // per-thread event buffer of the neuron kernel
+#define NEURON_BATCH 8         // event loads in flight per thread
 #define DEFAULT_EVENT_CAP 1024 // per-target event slots per step (capped by memory)
 
 // ------------------------------------------------------------------ errors
@@ -1090,19 +1091,32 @@ __global__ void __launch_bounds__(NEURON_BLOCK) neuron_kernel(Dev d) {
       float val[LOCAL_EVENTS];
       uint32_t key[LOCAL_EVENTS];
       const uint2 *ev = d.ev + (size_t)i * cap;
-      for (uint32_t e = 0; e < cnt; e++) {
-        const uint2 x = ev[e];
-        const double tm = event_time(d, x.x, t, D, N);
-        uint32_t p = e;
-        while (p > 0 && (tau[p - 1] > tm || (tau[p - 1] == tm && key[p - 1] > x.x))) {
-          tau[p] = tau[p - 1];
-          val[p] = val[p - 1];
-          key[p] = key[p - 1];
-          p--;
+      // events in groups of NEURON_BATCH: the loads, then the arrival-time
+      // gathers, are all in flight together; then insertion by (time, key)
+      for (uint32_t e0 = 0; e0 < cnt; e0 += NEURON_BATCH) {
+        uint2 x[NEURON_BATCH];
+        double tm[NEURON_BATCH];
+#pragma unroll
+        for (int u = 0; u < NEURON_BATCH; u++)
+          if (e0 + u < cnt) x[u] = ev[e0 + u];
+#pragma unroll
+        for (int u = 0; u < NEURON_BATCH; u++)
+          if (e0 + u < cnt) tm[u] = event_time(d, x[u].x, t, D, N);
+#pragma unroll
+        for (int u = 0; u < NEURON_BATCH; u++) {
+          if (e0 + u < cnt) {
+            uint32_t p = e0 + u;
+            while (p > 0 && (tau[p - 1] > tm[u] || (tau[p - 1] == tm[u] && key[p - 1] > x[u].x))) {
+              tau[p] = tau[p - 1];
+              val[p] = val[p - 1];
+              key[p] = key[p - 1];
+              p--;
+            }
+            tau[p] = tm[u];
+            val[p] = __uint_as_float(x[u].y);
+            key[p] = x[u].x;
+          }
         }
-        tau[p] = tm;
-        val[p] = __uint_as_float(x.y);
-        key[p] = x.x;
       }
       fired = run_neuron(d, i, t, tau, val, cnt);
     }
@@ -1129,22 +1143,21 @@ __device__ static inline void bitonic_sort_shared(double *tau, uint32_t *key, fl
                                                   uint32_t tid, uint32_t nthr, bool warp_only) {
   for (uint32_t k = 2; k <= n2; k <<= 1) {
     for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-      for (uint32_t a = tid; a < n2; a += nthr) {
-        const uint32_t b = a ^ j;
-        if (b > a) {
-          const bool up = (a & k) == 0;
-          const double ta = tau[a], tb = tau[b];
-          const uint32_t ka = key[a], kb = key[b];
-          const bool gt = (ta > tb) || (ta == tb && ka > kb);
-          if (gt == up) {
-            tau[a] = tb;
-            tau[b] = ta;
-            key[a] = kb;
-            key[b] = ka;
-            const float va = val[a];
-            val[a] = val[b];
-            val[b] = va;
-          }
+      // pair p compares a = p with bit j inserted as 0, and b = a | j
+      for (uint32_t p = tid; p < (n2 >> 1); p += nthr) {
+        const uint32_t a = ((p & ~(j - 1)) << 1) | (p & (j - 1)), b = a | j;
+        const bool up = (a & k) == 0;
+        const double ta = tau[a], tb = tau[b];
+        const uint32_t ka = key[a], kb = key[b];
+        const bool gt = (ta > tb) || (ta == tb && ka > kb);
+        if (gt == up) {
+          tau[a] = tb;
+          tau[b] = ta;
+          key[a] = kb;
+          key[b] = ka;
+          const float va = val[a];
+          val[a] = val[b];
+          val[b] = va;
         }
       }
       if (warp_only) __syncwarp(); else __syncthreads();
@@ -1153,8 +1166,10 @@ __device__ static inline void bitonic_sort_shared(double *tau, uint32_t *key, fl
 }
 
 // Events per neuron handled by the warp path: at most the bucket size.
+// (the sorted times and weights are written back into the first half and
+// the second half of the bucket)
 __device__ static inline uint32_t warp_path_max(const NetConst *net) {
-  return min(net->ev_cap, (uint32_t)HEAVY_WARP_MAX);
+  return min(net->ev_cap / 2, (uint32_t)HEAVY_WARP_MAX);
 }
 
 __global__ void __launch_bounds__(HEAVY_SORT_WARPS * 32) heavy_sort_kernel(Dev d) {
@@ -1188,13 +1203,19 @@ __global__ void __launch_bounds__(HEAVY_SORT_WARPS * 32) heavy_sort_kernel(Dev d
     }
     __syncwarp();
     bitonic_sort_shared(tau, key, val, n2, lane, 32, true);
-    for (uint32_t e = lane; e < n; e += 32) ev[e] = make_uint2(key[e], __float_as_uint(val[e]));
+    // sorted arrival times into the bucket's first half, weights into its second
+    double *st = reinterpret_cast<double *>(ev);
+    float *sv = reinterpret_cast<float *>(ev + cap / 2);
+    for (uint32_t e = lane; e < n; e += 32) {
+      st[e] = tau[e];
+      sv[e] = val[e];
+    }
     __syncwarp();
   }
 }
 
-// Runs a neuron whose events sit sorted in its bucket (arrival times are
-// recomputed from the keys); same merge and arithmetic as run_neuron.
+// Runs a neuron whose events heavy_sort_kernel left sorted in its bucket
+// (arrival times, then weights); same merge and arithmetic as run_neuron.
 __global__ void heavy_run_kernel(Dev d) {
   const NetConst *net = d.net;
   const uint32_t t = *d.t, N = net->N, D = net->D, cap = net->ev_cap, wmax = warp_path_max(net);
@@ -1203,6 +1224,8 @@ __global__ void heavy_run_kernel(Dev d) {
     const uint32_t i = d.heavy_list[hh], ns = d.heavy_list[N + hh];
     if (ns > wmax) continue;
     const uint2 *ev = d.ev + (size_t)i * cap;
+    const double *st = reinterpret_cast<const double *>(ev);
+    const float *sv = reinterpret_cast<const float *>(ev + cap / 2);
     const uint32_t s = d.sub[i];
     NeuronRegs n;
     n.v = d.v[i];
@@ -1216,17 +1239,17 @@ __global__ void heavy_run_kernel(Dev d) {
     const double *lut = d.lut + (size_t)s * 256;
     uint32_t a = 0, b = 0;
     double bt = (b < bc) ? d.bath_time[bbase] : 0.0;
-    uint2 x = ev[0];
-    double at = event_time(d, x.x, t, D, N);
+    double at = st[0];
+    float aw = sv[0];
     while (a < ns || b < bc) {
       double ct, I;
       if (a < ns && (b >= bc || at <= bt)) {
         ct = at;
-        I = (double)__uint_as_float(x.y);
+        I = (double)aw;
         a++;
         if (a < ns) {
-          x = ev[a];
-          at = event_time(d, x.x, t, D, N);
+          at = st[a];
+          aw = sv[a];
         }
       } else {
         ct = bt;
