@@ -383,7 +383,8 @@ struct Dev {
   uint2 *ev;
   uint32_t *ovf_cnt;
   uint4 *ovf;
-  uint32_t *heavy_list, *heavy_cnt;   // [2N]: neuron, event count
+  uint32_t *heavy_list, *heavy_cnt;   // [4N]: neuron, event count of the warp path, then of
+                                      // the block path; heavy_cnt[0..1]: their lengths
   // bath
   uint32_t *bath_hist;      // [P][64] ran3 history ring
   uint64_t *bath_produced, *bath_pos;  // [P]
@@ -1072,6 +1073,8 @@ __device__ static inline int run_neuron(const Dev &d, uint32_t i, uint32_t t, co
 // Light neurons (at most LOCAL_EVENTS synaptic events this step): one thread
 // each, insertion sort by (arrival time, key) in registers/local memory.
 // Heavier neurons are queued for the heavy path below.
+__device__ static inline uint32_t warp_path_max(const NetConst *net);
+
 __global__ void __launch_bounds__(NEURON_BLOCK) neuron_kernel(Dev d) {
   const NetConst *net = d.net;
   const uint32_t t = *d.t, N = net->N, D = net->D, cap = net->ev_cap;
@@ -1081,10 +1084,11 @@ __global__ void __launch_bounds__(NEURON_BLOCK) neuron_kernel(Dev d) {
     const uint32_t cnt = d.ev_cnt[i];
     d.ev_cnt[i] = 0;
     if (cnt > LOCAL_EVENTS) {
-      uint32_t k = atomicAdd(d.heavy_cnt, 1u);
+      const uint32_t path = (cnt <= warp_path_max(net)) ? 0u : 1u;
+      const uint32_t k = atomicAdd(&d.heavy_cnt[path], 1u);
       if (k < N) {
-        d.heavy_list[k] = i;
-        d.heavy_list[N + k] = cnt;
+        d.heavy_list[2ull * N * path + k] = i;
+        d.heavy_list[2ull * N * path + N + k] = cnt;
       }
     } else {
       double tau[LOCAL_EVENTS];
@@ -1183,10 +1187,10 @@ __global__ void __launch_bounds__(HEAVY_SORT_WARPS * 32) heavy_sort_kernel(Dev d
   double *tau = tau_base + (size_t)w * HEAVY_WARP_MAX;
   uint32_t *key = key_base + (size_t)w * HEAVY_WARP_MAX;
   float *val = val_base + (size_t)w * HEAVY_WARP_MAX;
-  const uint32_t nh = min(*d.heavy_cnt, N);
+  const uint32_t nh = min(d.heavy_cnt[0], N);
   for (uint32_t hh = blockIdx.x * HEAVY_SORT_WARPS + w; hh < nh; hh += gridDim.x * HEAVY_SORT_WARPS) {
     const uint32_t i = d.heavy_list[hh], n = d.heavy_list[N + hh];
-    if (n > wmax) continue;   // huge_kernel
+    if (n > wmax) continue;   // not listed here
     uint2 *ev = d.ev + (size_t)i * cap;
     uint32_t n2 = 1;
     while (n2 < n) n2 <<= 1;
@@ -1219,7 +1223,7 @@ __global__ void __launch_bounds__(HEAVY_SORT_WARPS * 32) heavy_sort_kernel(Dev d
 __global__ void heavy_run_kernel(Dev d) {
   const NetConst *net = d.net;
   const uint32_t t = *d.t, N = net->N, D = net->D, cap = net->ev_cap, wmax = warp_path_max(net);
-  const uint32_t nh = min(*d.heavy_cnt, N);
+  const uint32_t nh = min(d.heavy_cnt[0], N);
   for (uint32_t hh = blockIdx.x * blockDim.x + threadIdx.x; hh < nh; hh += gridDim.x * blockDim.x) {
     const uint32_t i = d.heavy_list[hh], ns = d.heavy_list[N + hh];
     if (ns > wmax) continue;
@@ -1308,10 +1312,11 @@ __global__ void __launch_bounds__(HEAVY_THREADS) huge_kernel(Dev d) {
   __shared__ uint32_t s_n;
   const NetConst *net = d.net;
   const uint32_t t = *d.t, N = net->N, D = net->D, tid = threadIdx.x;
-  const uint32_t nh = min(*d.heavy_cnt, N);
+  const uint32_t nh = min(d.heavy_cnt[1], N);
+  const uint32_t *hl = d.heavy_list + 2ull * N;
   for (uint32_t hh = blockIdx.x; hh < nh; hh += gridDim.x) {
-    const uint32_t i = d.heavy_list[hh], cnt = d.heavy_list[N + hh];
-    if (cnt <= warp_path_max(net)) continue;
+    const uint32_t i = hl[hh], cnt = hl[N + hh];
+    if (cnt <= warp_path_max(net)) continue;   // not listed here
     if (cnt > MAX_INPUTS_PER_STEP) {
       if (tid == 0) atomicOr(d.flags, F_TOO_MANY_INPUTS);
       continue;
@@ -1373,7 +1378,8 @@ __global__ void ltp_kernel(Dev d) {
 
 __global__ void end_step_kernel(Dev d) {
   *d.ovf_cnt = 0;
-  *d.heavy_cnt = 0;
+  d.heavy_cnt[0] = 0;
+  d.heavy_cnt[1] = 0;
   *d.t = *d.t + 1;
 }
 
@@ -1469,6 +1475,7 @@ struct dpsnn_engine {
   uint64_t launches = 0;               // kernels enqueued by dpsnn_step
   std::vector<float> fix_vals;
   std::vector<uint32_t> fix_keys, fix_bucket;
+  uint32_t *h_pin = nullptr;          // pinned {flags, spike count} for per-step reads
 };
 
 static void collect_timings(dpsnn_engine *e);
@@ -1870,8 +1877,8 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
   DALLOC(d.ev, (size_t)N * n.ev_cap);
   DALLOC(d.ovf_cnt, 1);
   DALLOC(d.ovf, n.ovf_cap);
-  DALLOC(d.heavy_list, 2ull * N);
-  DALLOC(d.heavy_cnt, 1);
+  DALLOC(d.heavy_list, 4ull * N);
+  DALLOC(d.heavy_cnt, 2);
   DALLOC(d.t, 1);
   DALLOC(d.flags, 4);
   DALLOC(d.events, 1);
@@ -1988,6 +1995,7 @@ extern "C" int dpsnn_create(const dpsnn_params *p, const dpsnn_options *opts, dp
     ok = cudaEventCreateWithFlags(&e->ev_bath[b], cudaEventDisableTiming) == cudaSuccess &&
          cudaEventCreateWithFlags(&e->ev_neuron[b], cudaEventDisableTiming) == cudaSuccess;
   ok = ok && cudaEventCreateWithFlags(&e->ev_start, cudaEventDisableTiming) == cudaSuccess;
+  ok = ok && cudaMallocHost((void **)&e->h_pin, 2 * sizeof(uint32_t)) == cudaSuccess;
   if (!ok) {
     const int dev = e->device;
     dpsnn_destroy(e);
@@ -2015,15 +2023,20 @@ extern "C" void dpsnn_destroy(dpsnn_engine *e) {
     if (e->ev_neuron[b]) cudaEventDestroy(e->ev_neuron[b]);
   }
   if (e->ev_start) cudaEventDestroy(e->ev_start);
+  if (e->h_pin) cudaFreeHost(e->h_pin);
   if (e->bath_stream) cudaStreamDestroy(e->bath_stream);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
 }
 
+static int flags_error(uint32_t f);
 static int check_flags(dpsnn_engine *e) {
   uint32_t f = 0;
   CK(cudaMemcpyAsync(&f, e->d.flags, 4, cudaMemcpyDeviceToHost, e->stream));
   CK(cudaStreamSynchronize(e->stream));
+  return flags_error(f);
+}
+static int flags_error(uint32_t f) {
   if (!f) return 0;
   if (f & F_TIME_WINDOW) return dpsnn_fail(DPSNN_E_MODEL, "ERROR in neu dynamic: input currentTime in wrong ms");
   if (f & F_NO_TARGET) return dpsnn_fail(DPSNN_E_MODEL, "ERROR neuSpikToAxSp: no forw host targ for a spiking neuron");
@@ -2181,16 +2194,24 @@ extern "C" uint64_t dpsnn_events_delivered(const dpsnn_engine *e) {
 extern "C" int dpsnn_spikes(dpsnn_engine *e, uint32_t t_ms, uint32_t *ids, double *te, uint32_t cap,
                             uint32_t *count) {
   if (!e || !count) return dpsnn_fail(DPSNN_E_PARAM, "null argument");
-  int rc = dpsnn_sync(e);
-  if (rc) return rc;
   if (t_ms >= e->t_host || t_ms + RING_SLOTS <= e->t_host)
     return dpsnn_fail(DPSNN_E_STATE, "step %u is not among the last %d completed steps", t_ms, RING_SLOTS);
-  uint32_t slot = t_ms % RING_SLOTS, cnt = 0;
-  CK(cudaMemcpy(&cnt, e->d.ring_cnt + slot, 4, cudaMemcpyDeviceToHost));
+  cudaSetDevice(e->device);
+  const uint32_t slot = t_ms % RING_SLOTS;
+  // one round trip for the error flags and the count, one for the list
+  CK(cudaMemcpyAsync(e->h_pin, e->d.flags, 4, cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaMemcpyAsync(e->h_pin + 1, e->d.ring_cnt + slot, 4, cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  int rc = flags_error(e->h_pin[0]);
+  if (rc) return rc;
+  const uint32_t cnt = e->h_pin[1];
   *count = cnt;
-  uint32_t k = std::min(cnt, cap);
-  if (k && ids) CK(cudaMemcpy(ids, e->d.ring_ids + (size_t)slot * e->hnet.N, 4ull * k, cudaMemcpyDeviceToHost));
-  if (k && te) CK(cudaMemcpy(te, e->d.ring_te + (size_t)slot * e->hnet.N, 8ull * k, cudaMemcpyDeviceToHost));
+  const uint32_t k = std::min(cnt, cap);
+  if (k && ids)
+    CK(cudaMemcpyAsync(ids, e->d.ring_ids + (size_t)slot * e->hnet.N, 4ull * k, cudaMemcpyDeviceToHost, e->stream));
+  if (k && te)
+    CK(cudaMemcpyAsync(te, e->d.ring_te + (size_t)slot * e->hnet.N, 8ull * k, cudaMemcpyDeviceToHost, e->stream));
+  if (k && (ids || te)) CK(cudaStreamSynchronize(e->stream));
   return 0;
 }
 

@@ -211,14 +211,15 @@ class Engine:
         return self._L.dpsnn_events_delivered(self._h)
 
     def spikes(self, t_ms: int):
+        """(ids, emission times) of the spikes detected at step t_ms."""
+        if getattr(self, "_sbuf", None) is None:
+            self._sbuf = (np.empty(self.glob_n, np.uint32), np.empty(self.glob_n, np.float64))
+        ids, te = self._sbuf
         cnt = C.c_uint32()
-        self._check(self._L.dpsnn_spikes(self._h, t_ms, None, None, 0, C.byref(cnt)), "dpsnn_spikes")
+        self._check(self._L.dpsnn_spikes(self._h, t_ms, _ptr(ids), _ptr(te), self.glob_n, C.byref(cnt)),
+                    "dpsnn_spikes")
         n = cnt.value
-        ids = np.empty(n, np.uint32)
-        te = np.empty(n, np.float64)
-        if n:
-            self._check(self._L.dpsnn_spikes(self._h, t_ms, _ptr(ids), _ptr(te), n, C.byref(cnt)), "dpsnn_spikes")
-        return ids, te
+        return ids[:n].copy(), te[:n].copy()
 
     def rank_spikes_noalloc(self, t_ms: int, rank: int):
         """Spikes of one emulated rank at step t_ms, gathered without any

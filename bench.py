@@ -299,7 +299,7 @@ def main():
     for k in range(e2e_steps):
         eng.step(1)
         ids, te = eng.spikes(args.warmup + k)
-        d2h += ids.nbytes + te.nbytes + 4
+        d2h += ids.nbytes + te.nbytes + 8   # + error flags and count
     h1 = time.perf_counter()
     e2e_events = eng.events_delivered() - ee0
     e2e_val = all_sum(e2e_events) / all_max(h1 - h0)
