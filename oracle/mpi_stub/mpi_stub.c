@@ -35,12 +35,16 @@ double MPI_Wtime(void) {
 int MPI_Get_address(const void *loc, MPI_Aint *addr) { *addr = (MPI_Aint)loc; return 0; }
 int MPI_Type_create_struct(int count, const int bl[], const MPI_Aint disp[],
                            const MPI_Datatype types[], MPI_Datatype *nt) {
-  MPI_Aint ext = 0;
+  /* extent padded to the largest member alignment, as MPI does */
+  MPI_Aint ext = 0, align = 1;
   for (int i = 0; i < count; i++) {
-    MPI_Aint end = disp[i] + (MPI_Aint)bl[i] * (MPI_Aint)type_size(types[i]);
+    const MPI_Aint sz = (MPI_Aint)type_size(types[i]);
+    MPI_Aint end = disp[i] + (MPI_Aint)bl[i] * sz;
     if (end > ext) ext = end;
+    const MPI_Aint a = sz >= 8 ? 8 : (sz >= 4 ? 4 : (sz >= 2 ? 2 : 1));
+    if (a > align) align = a;
   }
-  ext = (ext + 7) & ~(MPI_Aint)7;
+  ext = (ext + align - 1) & ~(align - 1);
   if (g_struct_count >= MAX_STRUCT_TYPES) unreachable("more struct types");
   g_struct_extent[g_struct_count] = ext;
   *nt = -(MPI_Datatype)(++g_struct_count);

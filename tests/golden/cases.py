@@ -18,4 +18,9 @@ CASES = {
     "small_2x2_stdp": lambda: small(2, 2, ms=2100, stdp=True, start_plasticity_ms=0),
     # the 2x2 benchmark network: 5000 neurons, ~5.6 M synapses, 1 s
     "c1_2x2": lambda: nc.cortical_grid(2, 2, total_ms=1000),
+    # several MPI ranks (env_globH), run by the reference as that many
+    # processes: each rank's own RNG streams, synapse lists and files
+    "small_2x2_p4": lambda: small(2, 2, seed=7, glob_h=4),
+    "small_2x2_stdp_p2": lambda: small(2, 2, ms=2100, stdp=True, start_plasticity_ms=0, glob_h=2),
+    "c1_2x2_p4": lambda: nc.cortical_grid(2, 2, total_ms=1000, glob_h=4),
 }

@@ -24,6 +24,15 @@ def raster(name):
     return np.array(ids, np.uint32), np.array(ts, np.float64)
 
 
+def rank_major(ids, ts, glob_h, glob_n):
+    """Reorder a step-major raster (every rank's spikes of a step, then the
+    next step) into the order of the reference's per-rank files read one
+    rank after the other."""
+    rank = ids // (glob_n // glob_h)
+    o = np.argsort(rank, kind="stable")
+    return ids[o], ts[o]
+
+
 def kat():
     out = {}
     with open(os.path.join(HERE, "ref_kat.txt")) as f:

@@ -8,7 +8,9 @@ built from the unmodified sources plus the bounds fix:
 
 * ``ref_kat.txt``        ran3 / NormDev / Gaussian LUT / roundr2i values from
                           the reference's own randdev.o and erflib.o;
-* ``<case>.raster.gz``   full-precision raster (%.17g) of the reference;
+* ``<case>.raster.gz``   full-precision raster (%.17g) of the reference, rank
+                          by rank when it runs several ranks (env_globH > 1,
+                          one process per rank over oracle/mpi_shm);
 * ``<case>.spikes.gz``   the reference's own spikes file (%.7g);
 * ``manifest.json``      sha256 of the BACKWARD synapse dump and of the
                           output files (spikes, ratesPerPop,
@@ -36,6 +38,9 @@ from tests.golden.cases import CASES  # noqa: E402
 nc = importlib.import_module("201812realtimecortsim_b200.netconfig")
 REF_HP = os.path.join(ROOT, "oracle", "_ref", "dpsnn_ref_hp")
 REF = os.path.join(ROOT, "oracle", "_ref", "dpsnn_ref")
+# the same reference objects over the shared-memory MPI subset, for env_globH > 1
+REF_MP_HP = os.path.join(ROOT, "oracle", "_ref", "dpsnn_ref_mp_hp")
+REF_MP = os.path.join(ROOT, "oracle", "_ref", "dpsnn_ref_mp")
 KAT = os.path.join(ROOT, "oracle", "_ref", "ref_kat")
 
 
@@ -55,13 +60,16 @@ def gz_text(path):
 def run(binary, cfg, workdir):
     env = dict(os.environ)
     env.update(cfg.write(workdir))
+    if cfg.glob_h > 1:   # one process per rank
+        binary = {REF_HP: REF_MP_HP, REF: REF_MP}[binary]
+        env["DPSNN_SHM_RANKS"] = str(cfg.glob_h)
     r = subprocess.run([binary], cwd=workdir, env=env, capture_output=True, text=True)
     if r.returncode != 0 or "ERROR" in r.stdout:
         raise RuntimeError(r.stdout[-2000:] + r.stderr[-2000:])
 
 
 def main():
-    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", "kat"], check=True,
+    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", "kat", "mp"], check=True,
                    capture_output=True)
     with open(os.path.join(HERE, "ref_kat.txt"), "w") as f:
         f.write(subprocess.run([KAT], check=True, capture_output=True, text=True).stdout)
@@ -75,12 +83,13 @@ def main():
             dump = [f for f in os.listdir(hp) if "SynapticList_BACKWARD" in f][0]
             entry["backward_dump"] = dump
             entry["backward_sha256"] = sha256(os.path.join(hp, dump))
-            lines = []
-            for sec in range((cfg.total_ms + 999) // 1000):
-                fn = os.path.join(hp, f"spikes-sec{sec}-C{cfg.n_modules}-H{cfg.glob_h}-h000.dat")
-                if os.path.exists(fn):
-                    with open(fn) as f:
-                        lines += f.readlines()
+            lines = []   # rank-major: all of rank 0's lines, then rank 1's, ...
+            for h in range(cfg.glob_h):
+                for sec in range((cfg.total_ms + 999) // 1000):
+                    fn = os.path.join(hp, f"spikes-sec{sec}-C{cfg.n_modules}-H{cfg.glob_h}-h{h:03d}.dat")
+                    if os.path.exists(fn):
+                        with open(fn) as f:
+                            lines += f.readlines()
             entry["spikes"] = len(lines)
             with gz_text(os.path.join(HERE, f"{name}.raster.gz")) as f:
                 f.writelines(lines)
@@ -92,8 +101,9 @@ def main():
                     outs[fn] = sha256(os.path.join(std, fn))
             entry["outputs_sha256"] = outs
             with gz_text(os.path.join(HERE, f"{name}.spikes.gz")) as f:
-                with open(os.path.join(std, f"spikes-sec0-C{cfg.n_modules}-H{cfg.glob_h}-h000.dat")) as g:
-                    f.write(g.read())
+                for h in range(cfg.glob_h):
+                    with open(os.path.join(std, f"spikes-sec0-C{cfg.n_modules}-H{cfg.glob_h}-h{h:03d}.dat")) as g:
+                        f.write(g.read())
         # synaptic events delivered in the run (identical dynamics in the
         # restatement, pinned by the raster and dump checks)
         sys.path.insert(0, os.path.join(ROOT, "oracle"))

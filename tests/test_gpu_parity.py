@@ -32,6 +32,7 @@ def run_engine(cfg, steps, chunk=50):
 def test_raster_identical_to_reference(name):
     cfg = CASES[name]()
     eng, ids, ts = run_engine(cfg, cfg.total_ms)
+    ids, ts = gio.rank_major(ids, ts, cfg.glob_h, eng.glob_n)
     gi, gt = gio.raster(name)
     assert len(ids) == len(gi)
     np.testing.assert_array_equal(ids, gi)

@@ -76,8 +76,9 @@ def test_raster_matches_reference(name):
         ids.append(i)
         ts.append(t)
     gi, gt = gio.raster(name)
-    np.testing.assert_array_equal(np.concatenate(ids), gi)
-    np.testing.assert_array_equal(np.concatenate(ts), gt)
+    ids, ts = gio.rank_major(np.concatenate(ids), np.concatenate(ts), cfg.glob_h, net.glob_n)
+    np.testing.assert_array_equal(ids, gi)
+    np.testing.assert_array_equal(ts, gt)
 
 
 def test_correctly_rounded_libm_matches_system_on_2x2():
