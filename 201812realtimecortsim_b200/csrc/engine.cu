@@ -101,6 +101,8 @@ struct NetConst {
   float stdp_drift, stdp_tauDecay;
   uint32_t ev_cap, ovf_cap;
   uint32_t bath_need;  // largest maxExternCurrentCount
+  uint32_t delay_exp;  // getRandomDelay_EXP instead of _UNI
+  float inv_log_tn;    // (float)(1.0 / log(0.05)), the EXP tail constant
 };
 
 // ------------------------------------------------------------------ ran3
@@ -242,6 +244,32 @@ __device__ static inline uint32_t random_delay_uni(const NetConst *net, Ran3 &g,
   return roundr2i(outF * DelayStep);
 }
 
+// getRandomDelay_EXP (DPSNN_LIFCAcorticalModuleGen.cpp:247-297), the
+// reference Makefile's default: a truncated exponential over [DMin, DMax);
+// 0xFFFFFFFF where the reference stops with an error.
+__device__ static inline uint32_t random_delay_exp(const NetConst *net, Ran3 &g, uint32_t s, uint32_t t) {
+  float outfuncF, DMin, DMax, DelayMin, DelayMax, DelayStep, DelayNum;
+  const float InvLogTN = net->inv_log_tn;
+  DMin = (float)net->DMin[s * DPSNN_MAX_SUBPOP + t];
+  DMax = (float)net->DMax[s * DPSNN_MAX_SUBPOP + t];
+  DelayMin = (float)net->delay_min;
+  DelayMax = (float)net->delay_max;
+  DelayNum = 80;
+  DelayStep = (DelayMax - DelayMin) / DelayNum;
+  DelayMax -= DelayStep / 2;
+  DelayMin += DelayStep / 2;
+  DMax = roundr2i((DMax - DelayMin) / DelayStep) * DelayStep + DelayMin;
+  DMin = roundr2i((DMin - DelayMin) / DelayStep) * DelayStep + DelayMin;
+  outfuncF = (float)((((double)DMin + (double)(DMax - DMin - DelayStep) *
+                       log_cr(1.0 - r3_rand(g) * (1.0 - 0.05)) * (double)InvLogTN) -
+                      (double)DelayMin) / (double)DelayStep);
+  if (outfuncF >= DelayNum) return 0xFFFFFFFFu;
+  const uint32_t outfunc = roundr2i(outfuncF * DelayStep);
+  if (outfunc >= net->DMax[s * DPSNN_MAX_SUBPOP + t]) return 0xFFFFFFFFu;
+  (void)DelayMax;
+  return outfunc;
+}
+
 __global__ void gen_kernel(const NetConst *__restrict__ net, const float *__restrict__ prob, int pass,
                            GenRecord *rec, const int32_t *__restrict__ chosen_hyp,
                            const double *__restrict__ chosen_cache, uint16_t *cnt_out,
@@ -299,7 +327,7 @@ __global__ void gen_kernel(const NetConst *__restrict__ net, const float *__rest
     for (uint32_t j = 0; j < tot; j++) {
       uint32_t tg = tl[j];
       uint32_t tsub = subpop_of(net, tg % npcm);
-      uint32_t delay = random_delay_uni(net, g, ssub, tsub);
+      uint32_t delay = net->delay_exp ? random_delay_exp(net, g, ssub, tsub) : random_delay_uni(net, g, ssub, tsub);
       if (delay >= D) { R->err = GEN_ERR_DELAY; R->err_arg = delay; return; }
       float mean = (float)net->J[ssub * DPSNN_MAX_SUBPOP + tsub];
       float sigma = (float)(net->DJ[ssub * DPSNN_MAX_SUBPOP + tsub] * (double)mean);
@@ -1651,6 +1679,8 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
       }
     n.delay_min = (uint32_t)dmin;
     n.delay_max = (uint32_t)dmax;
+    n.delay_exp = p->delay_exponential ? 1u : 0u;
+    n.inv_log_tn = (float)(1.0 / log_cr(0.05));
   }
   if (!(p->min_syn_weight_f < 0) || p->min_syn_weight_f < -6.0f)
     return dpsnn_fail(DPSNN_E_PARAM, "env_minSynWeigth out of range -6.000000 - 0.0");

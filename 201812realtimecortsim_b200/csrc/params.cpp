@@ -188,6 +188,13 @@ extern "C" int dpsnn_params_from_env(const char *workdir, dpsnn_params *p) {
   s = getenv("env_howManyOutputFiles");
   p->howManyOutputFiles = s ? (uint32_t)atoi(s) : 0;
   if (p->howManyOutputFiles > 1) p->howManyOutputFiles = 0;
+  // the delay distribution is a compile-time choice in the reference
+  // (-DDelayUniform, DPSNN_LIFCAcorticalModuleGen.cpp:133-137)
+  s = getenv("DPSNN_DELAY_DISTRIBUTION");
+  p->delay_exponential = 0;
+  if (s && strcmp(s, "exponential") == 0) p->delay_exponential = 1;
+  else if (s && strcmp(s, "uniform") != 0)
+    return dpsnn_fail(DPSNN_E_PARAM, "DPSNN_DELAY_DISTRIBUTION must be uniform or exponential");
   if ((rc = env_u32("env_collectivesAlgo", &tmp))) return rc;
   if ((rc = env_u32("env_pktLength", &tmp))) return rc;
 

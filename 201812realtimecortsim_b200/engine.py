@@ -42,6 +42,7 @@ class Params(C.Structure):
         ("startRatesPerPop_s", C.c_uint32), ("stopRatesPerPop_s", C.c_uint32),
         ("spikes_writeDisable", C.c_uint32), ("statRatesPerPop_writeDisable", C.c_uint32),
         ("howManyOutputFiles", C.c_uint32),
+        ("delay_exponential", C.c_uint32),
     ]
 
 
@@ -155,6 +156,7 @@ def params_from_netconfig(cfg) -> ParamsHolder:
     p.startStatFiles_s, p.stopStatFiles_s = 0, 100000
     p.startRatesPerPop_s, p.stopRatesPerPop_s = 0, 100000
     p.howManyOutputFiles = 1
+    p.delay_exponential = 1 if getattr(cfg, "delay_exponential", False) else 0
     return ParamsHolder(p, spec, bath)
 
 

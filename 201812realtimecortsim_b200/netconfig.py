@@ -69,6 +69,9 @@ class NetConfig:
     stdp: Optional[tuple] = None          # plasticity.txt row, or None
     start_plasticity_ms: int = 10 ** 8
     stop_plasticity_ms: int = 10 ** 8
+    # getRandomDelay_EXP instead of getRandomDelay_UNI: the reference picks it
+    # at compile time (no -DDelayUniform); the engine reads DPSNN_DELAY_DISTRIBUTION
+    delay_exponential: bool = False
     extra_env: Dict[str, str] = field(default_factory=dict)
 
     @property
@@ -145,6 +148,8 @@ class NetConfig:
             "env_collectivesAlgo": "0",
             "env_pktLength": "0",
         }
+        if self.delay_exponential:
+            e["DPSNN_DELAY_DISTRIBUTION"] = "exponential"
         e.update(self.extra_env)
         return e
 
@@ -212,7 +217,8 @@ def cortical_grid(cfx: int, cfy: int, *, mu: float = 0.3, g_c: float = 3.0,
                   stencil_dim: int = 2, p_intra: float = 0.8,
                   p1: Optional[float] = None, lam: float = 1.0,
                   total_ms: int = 1000, seed: int = 1, glob_h: int = 1,
-                  stdp: bool = False, start_plasticity_ms: int = 0) -> NetConfig:
+                  stdp: bool = False, start_plasticity_ms: int = 0,
+                  delay_exponential: bool = False) -> NetConfig:
     """The benchmark network family (see module docstring)."""
     if p1 is None:
         # 0.0376 at 2x2 reproduces the ~1125 in-degree of the 2x2 benchmark;
@@ -232,7 +238,7 @@ def cortical_grid(cfx: int, cfy: int, *, mu: float = 0.3, g_c: float = 3.0,
             conn[(s, t)] = (J, 0.1, 1.0, 20.0, probs)
     cfg = NetConfig(cfx=cfx, cfy=cfy, subpops=subpops, conn=conn,
                     stencil_dim=stencil_dim, total_ms=total_ms, seed=seed,
-                    glob_h=glob_h)
+                    glob_h=glob_h, delay_exponential=delay_exponential)
     if stdp:
         cfg.stdp = (1, -1, 0.1, 20, 0.1, 0.12, 1, 0)
         cfg.start_plasticity_ms = start_plasticity_ms

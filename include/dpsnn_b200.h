@@ -80,6 +80,10 @@ typedef struct {
   uint32_t moduloSec, ratesSampling, startStatFiles_s, stopStatFiles_s;
   uint32_t startRatesPerPop_s, stopRatesPerPop_s;
   uint32_t spikes_writeDisable, statRatesPerPop_writeDisable, howManyOutputFiles;
+  /* 0: getRandomDelay_UNI (reference built with -DDelayUniform);
+   * 1: getRandomDelay_EXP (the reference Makefile's default).  The reference
+   * selects it at compile time; here DPSNN_DELAY_DISTRIBUTION=exponential. */
+  uint32_t delay_exponential;
 } dpsnn_params;
 
 /* Engine capacities (0 = default). */

@@ -295,6 +295,35 @@ static uint32_t random_delay_uni(dpo_net *n, o_rng *g, uint32_t s, uint32_t t) {
   return dpo_roundr2i(outF * DelayStep);
 }
 
+/* getRandomDelay_EXP (DPSNN_LIFCAcorticalModuleGen.cpp:247-297): a truncated
+ * exponential over [DMin, DMax), float/double promotions as written there.
+ * The constant 1/log(0.05) is folded at compile time by the reference build,
+ * i.e. correctly rounded.  Returns 0xFFFFFFFF on the reference's error exits. */
+#define O_TAIL_NEGLECTED 0.05
+static uint32_t random_delay_exp(dpo_net *n, o_rng *g, uint32_t s, uint32_t t) {
+  float InvLogTN, outfuncF, DMin, DMax, DelayMin, DelayMax, DelayStep, DelayNum;
+  uint32_t outfunc;
+  DMin = (float)n->sp_DMin[s][t];
+  DMax = (float)n->sp_DMax[s][t];
+  DelayMin = (float)n->delay_min;
+  DelayMax = (float)n->delay_max;
+  DelayNum = 80;
+  InvLogTN = (float)(1.0 / dpo_log_cr(O_TAIL_NEGLECTED));
+  DelayStep = (DelayMax - DelayMin) / DelayNum;
+  DelayMax -= DelayStep / 2;
+  DelayMin += DelayStep / 2;
+  DMax = dpo_roundr2i((DMax - DelayMin) / DelayStep) * DelayStep + DelayMin;
+  DMin = dpo_roundr2i((DMin - DelayMin) / DelayStep) * DelayStep + DelayMin;
+  outfuncF = (float)((((double)DMin + (double)(DMax - DMin - DelayStep) *
+                       o_log(1.0 - o_random(g) * (1.0 - O_TAIL_NEGLECTED)) * (double)InvLogTN) -
+                      (double)DelayMin) / (double)DelayStep);
+  if (outfuncF >= DelayNum) return 0xFFFFFFFFu;
+  outfunc = dpo_roundr2i(outfuncF * DelayStep);
+  if (outfunc >= n->sp_DMax[s][t]) return 0xFFFFFFFFu;
+  (void)DelayMax;
+  return outfunc;
+}
+
 typedef struct { uint32_t glob, host, sub; } o_target;
 
 static int generate(dpo_net *n, o_syn **gen_out, uint64_t **rank_gen_start_out) {
@@ -361,7 +390,13 @@ static int generate(dpo_net *n, o_syn **gen_out, uint64_t **rank_gen_start_out) 
         s.post = tl[j].glob;
         n->fwd_hosts[(size_t)gn * n->glob_h + tl[j].host]++;
         uint32_t tsub = tl[j].sub;
-        s.delay = (uint8_t)random_delay_uni(n, g, ssub, tsub);
+        if (n->cfg.delay_exp) {
+          const uint32_t dl = random_delay_exp(n, g, ssub, tsub);
+          if (dl == 0xFFFFFFFFu) { set_err("ERROR: delay level generated beyond the allowed delays"); return -1; }
+          s.delay = (uint8_t)dl;
+        } else {
+          s.delay = (uint8_t)random_delay_uni(n, g, ssub, tsub);
+        }
         s.kind = (uint8_t)ssub;
         float mean = (float)n->sp_J[ssub][tsub];
         float sigma = (float)n->sp_DJ[ssub][tsub] * mean;

@@ -15,7 +15,7 @@
  *   ran3 / SetRandomSeed / NormDev   randdev.c:116-196,477-502,584-606
  *   Gaussian LUT, roundr2i           erflib.c:41-181
  *   synapse generation               DPSNN_LIFCAcorticalModuleGen.cpp:62-220,
- *                                    :299-338; DPSNN_LIFCAconnectome.cpp:513-823,
+ *                                    :247-338; DPSNN_LIFCAconnectome.cpp:513-823,
  *                                    :871-887, :1079-1133
  *   connectome sort / offsets        DPSNN_localNet_init.c:311-740
  *   one 1 ms step                    DPSNN_localNet_sim.c:22-307, :620-999
@@ -59,6 +59,9 @@ typedef struct {
   /* plasticity.txt (defaults of readPlasticityParametersFile if absent) */
   float stdp_antiCausalCoeff, stdp_multiplier, stdp_tau_ms;
   float stdp_causalMax, stdp_antiCausalMax, stdp_tauDecay_s, stdp_drift;
+  /* delay distribution: 0 = getRandomDelay_UNI (built with -DDelayUniform),
+   * 1 = getRandomDelay_EXP (the reference Makefile's default) */
+  uint32_t delay_exp;
 } dpo_config;
 
 typedef struct dpo_net dpo_net;

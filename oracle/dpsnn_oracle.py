@@ -41,6 +41,7 @@ class DpoConfig(C.Structure):
         ("stdp_tau_ms", C.c_float), ("stdp_causalMax", C.c_float),
         ("stdp_antiCausalMax", C.c_float), ("stdp_tauDecay_s", C.c_float),
         ("stdp_drift", C.c_float),
+        ("delay_exp", C.c_uint32),
     ]
 
 
@@ -127,6 +128,7 @@ def config_from_netconfig(cfg) -> DpoConfig:
     c.stdp_antiCausalCoeff, c.stdp_multiplier, c.stdp_tau_ms = anti, mult, tau
     c.stdp_causalMax, c.stdp_antiCausalMax = cmax, amax
     c.stdp_tauDecay_s, c.stdp_drift = tdec, drift
+    c.delay_exp = 1 if getattr(cfg, "delay_exponential", False) else 0
     return c
 
 

@@ -23,4 +23,8 @@ CASES = {
     "small_2x2_p4": lambda: small(2, 2, seed=7, glob_h=4),
     "small_2x2_stdp_p2": lambda: small(2, 2, ms=2100, stdp=True, start_plasticity_ms=0, glob_h=2),
     "c1_2x2_p4": lambda: nc.cortical_grid(2, 2, total_ms=1000, glob_h=4),
+    # the reference Makefile's default delay distribution (getRandomDelay_EXP,
+    # built without -DDelayUniform)
+    "small_2x2_exp": lambda: small(2, 2, seed=7, delay_exponential=True),
+    "c1_2x2_exp": lambda: nc.cortical_grid(2, 2, total_ms=1000, delay_exponential=True),
 }

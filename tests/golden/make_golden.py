@@ -41,6 +41,9 @@ REF = os.path.join(ROOT, "oracle", "_ref", "dpsnn_ref")
 # the same reference objects over the shared-memory MPI subset, for env_globH > 1
 REF_MP_HP = os.path.join(ROOT, "oracle", "_ref", "dpsnn_ref_mp_hp")
 REF_MP = os.path.join(ROOT, "oracle", "_ref", "dpsnn_ref_mp")
+# built without -DDelayUniform: the reference Makefile's exponential delays
+REF_EXP_HP = os.path.join(ROOT, "oracle", "_ref", "dpsnn_ref_exp_hp")
+REF_EXP = os.path.join(ROOT, "oracle", "_ref", "dpsnn_ref_exp")
 KAT = os.path.join(ROOT, "oracle", "_ref", "ref_kat")
 
 
@@ -60,6 +63,8 @@ def gz_text(path):
 def run(binary, cfg, workdir):
     env = dict(os.environ)
     env.update(cfg.write(workdir))
+    if cfg.delay_exponential:
+        binary = {REF_HP: REF_EXP_HP, REF: REF_EXP}[binary]
     if cfg.glob_h > 1:   # one process per rank
         binary = {REF_HP: REF_MP_HP, REF: REF_MP}[binary]
         env["DPSNN_SHM_RANKS"] = str(cfg.glob_h)
@@ -69,7 +74,7 @@ def run(binary, cfg, workdir):
 
 
 def main():
-    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", "kat", "mp"], check=True,
+    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", "kat", "mp", "exp"], check=True,
                    capture_output=True)
     with open(os.path.join(HERE, "ref_kat.txt"), "w") as f:
         f.write(subprocess.run([KAT], check=True, capture_output=True, text=True).stdout)
