@@ -39,7 +39,7 @@ def test_raster_identical_to_reference(name):
     np.testing.assert_array_equal(ts, gt)
 
 
-@pytest.mark.parametrize("name", ["small_1x1", "small_2x2", "c1_2x2"])
+@pytest.mark.parametrize("name", ["small_1x1", "small_2x2", "c1_2x2", "c1_2x2_exp"])
 def test_connectome_identical_to_oracle(name):
     cfg = CASES[name]()
     eng = E.Engine(cfg)
