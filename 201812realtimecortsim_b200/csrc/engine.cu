@@ -1058,8 +1058,20 @@ __device__ static inline double event_time(const Dev &d, uint32_t key, uint32_t 
 // Runs the merged event sequence of one neuron: synaptic events (sorted by
 // (time, key)) merged with the bath events (time-ordered), synaptic first on
 // equal times (mergeFunction, DPSNN_neuron_sim.c:391-421, called at :644-646).
-__device__ static inline int run_neuron(const Dev &d, uint32_t i, uint32_t t, const double *tau,
-                                        const float *val, uint32_t ns) {
+// One event of a neuron's sort: one 16-byte load or store per element.
+struct __align__(16) SortEv {
+  double tau;
+  uint32_t key;
+  float val;
+};
+
+__device__ static inline bool sortev_gt(const SortEv &a, const SortEv &b) {
+  return (a.tau > b.tau) || (a.tau == b.tau && a.key > b.key);
+}
+
+
+template <typename Events>
+__device__ static inline int run_neuron_ev(const Dev &d, uint32_t i, uint32_t t, const Events &evs, uint32_t ns) {
   const NetConst *net = d.net;
   const uint32_t s = d.sub[i];
   NeuronRegs n;
@@ -1076,9 +1088,9 @@ __device__ static inline int run_neuron(const Dev &d, uint32_t i, uint32_t t, co
   double bt = (b < bc) ? d.bath_time[bbase] : 0.0;
   while (a < ns || b < bc) {
     double ct, I;
-    if (a < ns && (b >= bc || tau[a] <= bt)) {
-      ct = tau[a];
-      I = (double)val[a];
+    if (a < ns && (b >= bc || evs.time(a) <= bt)) {
+      ct = evs.time(a);
+      I = (double)evs.weight(a);
       a++;
     } else {
       ct = bt;
@@ -1095,6 +1107,26 @@ __device__ static inline int run_neuron(const Dev &d, uint32_t i, uint32_t t, co
   d.te[i] = n.te;
   if (n.fired) d.fired[i] = 1;
   return n.fired;
+}
+
+struct EvArrays {   // sorted times and weights in two arrays
+  const double *tau;
+  const float *val;
+  __device__ double time(uint32_t a) const { return tau[a]; }
+  __device__ float weight(uint32_t a) const { return val[a]; }
+};
+struct EvRecords {  // sorted 16-byte records
+  const SortEv *se;
+  __device__ double time(uint32_t a) const { return se[a].tau; }
+  __device__ float weight(uint32_t a) const { return se[a].val; }
+};
+
+__device__ static inline int run_neuron(const Dev &d, uint32_t i, uint32_t t, const double *tau,
+                                        const float *val, uint32_t ns) {
+  return run_neuron_ev(d, i, t, EvArrays{tau, val}, ns);
+}
+__device__ static inline int run_neuron_se(const Dev &d, uint32_t i, uint32_t t, const SortEv *se, uint32_t ns) {
+  return run_neuron_ev(d, i, t, EvRecords{se}, ns);
 }
 
 // Step 4: neuron update (regularDynamicTimeStep, DPSNN_neuron_sim.c:522-662).
@@ -1119,9 +1151,7 @@ __global__ void __launch_bounds__(NEURON_BLOCK) neuron_kernel(Dev d) {
         d.heavy_list[2ull * N * path + N + k] = cnt;
       }
     } else {
-      double tau[LOCAL_EVENTS];
-      float val[LOCAL_EVENTS];
-      uint32_t key[LOCAL_EVENTS];
+      SortEv se[LOCAL_EVENTS];
       const uint2 *ev = d.ev + (size_t)i * cap;
       // events in groups of NEURON_BATCH: the loads, then the arrival-time
       // gathers, are all in flight together; then insertion by (time, key)
@@ -1137,20 +1167,20 @@ __global__ void __launch_bounds__(NEURON_BLOCK) neuron_kernel(Dev d) {
 #pragma unroll
         for (int u = 0; u < NEURON_BATCH; u++) {
           if (e0 + u < cnt) {
+            SortEv y;
+            y.tau = tm[u];
+            y.key = x[u].x;
+            y.val = __uint_as_float(x[u].y);
             uint32_t p = e0 + u;
-            while (p > 0 && (tau[p - 1] > tm[u] || (tau[p - 1] == tm[u] && key[p - 1] > x[u].x))) {
-              tau[p] = tau[p - 1];
-              val[p] = val[p - 1];
-              key[p] = key[p - 1];
+            while (p > 0 && sortev_gt(se[p - 1], y)) {
+              se[p] = se[p - 1];
               p--;
             }
-            tau[p] = tm[u];
-            val[p] = __uint_as_float(x[u].y);
-            key[p] = x[u].x;
+            se[p] = y;
           }
         }
       }
-      fired = run_neuron(d, i, t, tau, val, cnt);
+      fired = run_neuron_se(d, i, t, se, cnt);
     }
   }
   const uint32_t bc = __syncthreads_count(fired);
@@ -1209,12 +1239,7 @@ __global__ void __launch_bounds__(HEAVY_SORT_WARPS * 32) heavy_sort_kernel(Dev d
   const NetConst *net = d.net;
   const uint32_t t = *d.t, N = net->N, D = net->D, cap = net->ev_cap, wmax = warp_path_max(net);
   const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  double *tau_base = reinterpret_cast<double *>(hs_raw);
-  uint32_t *key_base = reinterpret_cast<uint32_t *>(tau_base + HEAVY_SORT_WARPS * HEAVY_WARP_MAX);
-  float *val_base = reinterpret_cast<float *>(key_base + HEAVY_SORT_WARPS * HEAVY_WARP_MAX);
-  double *tau = tau_base + (size_t)w * HEAVY_WARP_MAX;
-  uint32_t *key = key_base + (size_t)w * HEAVY_WARP_MAX;
-  float *val = val_base + (size_t)w * HEAVY_WARP_MAX;
+  SortEv *se = reinterpret_cast<SortEv *>(hs_raw) + (size_t)w * HEAVY_WARP_MAX;
   const uint32_t nh = min(d.heavy_cnt[0], N);
   for (uint32_t hh = blockIdx.x * HEAVY_SORT_WARPS + w; hh < nh; hh += gridDim.x * HEAVY_SORT_WARPS) {
     const uint32_t i = d.heavy_list[hh], n = d.heavy_list[N + hh];
@@ -1223,24 +1248,41 @@ __global__ void __launch_bounds__(HEAVY_SORT_WARPS * 32) heavy_sort_kernel(Dev d
     uint32_t n2 = 1;
     while (n2 < n) n2 <<= 1;
     for (uint32_t e = lane; e < n2; e += 32) {
+      SortEv x;
       if (e < n) {
-        const uint2 x = ev[e];
-        key[e] = x.x;
-        val[e] = __uint_as_float(x.y);
-        tau[e] = event_time(d, x.x, t, D, N);
+        const uint2 r = ev[e];
+        x.tau = event_time(d, r.x, t, D, N);
+        x.key = r.x;
+        x.val = __uint_as_float(r.y);
       } else {
-        tau[e] = INFINITY;
-        key[e] = 0xFFFFFFFFu;
+        x.tau = INFINITY;
+        x.key = 0xFFFFFFFFu;
+        x.val = 0.0f;
       }
+      se[e] = x;
     }
     __syncwarp();
-    bitonic_sort_shared(tau, key, val, n2, lane, 32, true);
+    // bitonic network, pair p = (a with bit j cleared, a | j)
+    for (uint32_t k = 2; k <= n2; k <<= 1) {
+      for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+        for (uint32_t p = lane; p < (n2 >> 1); p += 32) {
+          const uint32_t a = ((p & ~(j - 1)) << 1) | (p & (j - 1)), b = a | j;
+          const SortEv xa = se[a], xb = se[b];
+          if (sortev_gt(xa, xb) == ((a & k) == 0)) {
+            se[a] = xb;
+            se[b] = xa;
+          }
+        }
+        __syncwarp();
+      }
+    }
     // sorted arrival times into the bucket's first half, weights into its second
     double *st = reinterpret_cast<double *>(ev);
     float *sv = reinterpret_cast<float *>(ev + cap / 2);
     for (uint32_t e = lane; e < n; e += 32) {
-      st[e] = tau[e];
-      sv[e] = val[e];
+      const SortEv x = se[e];
+      st[e] = x.tau;
+      sv[e] = x.val;
     }
     __syncwarp();
   }

@@ -157,6 +157,8 @@ def reference_processes() -> int:
     """One reference process per host thread, bounded by host memory
     (about 0.4 GB resident per process)."""
     n = os.cpu_count() or 1
+    if os.environ.get("DPSNN_BENCH_REF_PROCS"):   # a smaller sample (tests)
+        n = max(1, int(os.environ["DPSNN_BENCH_REF_PROCS"]))
     try:
         import psutil
         n = min(n, max(1, int(psutil.virtual_memory().available / 1.0e9)))
