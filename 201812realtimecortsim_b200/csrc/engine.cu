@@ -888,9 +888,9 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d, uint32_t t) {
           // lane L: the lapses at pos+1, pos+3, .., pos+1+2L, in 2^-20 units
           const uint32_t p32 = (uint32_t)pos;
           const uint32_t F = s.q[(p32 + 1 + 2 * lane) & M] - s.q[(p32 - 1) & M];
-          const uint32_t below = __ballot_sync(0xffffffffu, F < lo);
+          // F grows with L, so the lanes below the bounds are a prefix of m lanes
+          const uint32_t m = __reduce_add_sync(0xffffffffu, F < lo ? 1u : 0u);
           const uint32_t above = __ballot_sync(0xffffffffu, F >= hi1);
-          const uint32_t m = __popc(below);   // F grows with L: below is a prefix
           if (m < (misc & 0xFFu) && ((above >> m) & 1u)) {
             c = m + 1;
             pos += 2ull * c;
