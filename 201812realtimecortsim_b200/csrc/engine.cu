@@ -1058,7 +1058,9 @@ __device__ static inline double event_time(const Dev &d, uint32_t key, uint32_t 
 // Runs the merged event sequence of one neuron: synaptic events (sorted by
 // (time, key)) merged with the bath events (time-ordered), synaptic first on
 // equal times (mergeFunction, DPSNN_neuron_sim.c:391-421, called at :644-646).
-// One event of a neuron's sort: one 16-byte load or store per element.
+// One event of a light neuron's insertion sort (thread-local): one 16-byte
+// load or store per move.  The warp sorts keep separate arrays, whose 8- and
+// 4-byte shared accesses conflict less at the network's short strides.
 struct __align__(16) SortEv {
   double tau;
   uint32_t key;
@@ -1239,7 +1241,12 @@ __global__ void __launch_bounds__(HEAVY_SORT_WARPS * 32) heavy_sort_kernel(Dev d
   const NetConst *net = d.net;
   const uint32_t t = *d.t, N = net->N, D = net->D, cap = net->ev_cap, wmax = warp_path_max(net);
   const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  SortEv *se = reinterpret_cast<SortEv *>(hs_raw) + (size_t)w * HEAVY_WARP_MAX;
+  double *tau_base = reinterpret_cast<double *>(hs_raw);
+  uint32_t *key_base = reinterpret_cast<uint32_t *>(tau_base + HEAVY_SORT_WARPS * HEAVY_WARP_MAX);
+  float *val_base = reinterpret_cast<float *>(key_base + HEAVY_SORT_WARPS * HEAVY_WARP_MAX);
+  double *tau = tau_base + (size_t)w * HEAVY_WARP_MAX;
+  uint32_t *key = key_base + (size_t)w * HEAVY_WARP_MAX;
+  float *val = val_base + (size_t)w * HEAVY_WARP_MAX;
   const uint32_t nh = min(d.heavy_cnt[0], N);
   for (uint32_t hh = blockIdx.x * HEAVY_SORT_WARPS + w; hh < nh; hh += gridDim.x * HEAVY_SORT_WARPS) {
     const uint32_t i = d.heavy_list[hh], n = d.heavy_list[N + hh];
@@ -1248,41 +1255,24 @@ __global__ void __launch_bounds__(HEAVY_SORT_WARPS * 32) heavy_sort_kernel(Dev d
     uint32_t n2 = 1;
     while (n2 < n) n2 <<= 1;
     for (uint32_t e = lane; e < n2; e += 32) {
-      SortEv x;
       if (e < n) {
-        const uint2 r = ev[e];
-        x.tau = event_time(d, r.x, t, D, N);
-        x.key = r.x;
-        x.val = __uint_as_float(r.y);
+        const uint2 x = ev[e];
+        key[e] = x.x;
+        val[e] = __uint_as_float(x.y);
+        tau[e] = event_time(d, x.x, t, D, N);
       } else {
-        x.tau = INFINITY;
-        x.key = 0xFFFFFFFFu;
-        x.val = 0.0f;
+        tau[e] = INFINITY;
+        key[e] = 0xFFFFFFFFu;
       }
-      se[e] = x;
     }
     __syncwarp();
-    // bitonic network, pair p = (a with bit j cleared, a | j)
-    for (uint32_t k = 2; k <= n2; k <<= 1) {
-      for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-        for (uint32_t p = lane; p < (n2 >> 1); p += 32) {
-          const uint32_t a = ((p & ~(j - 1)) << 1) | (p & (j - 1)), b = a | j;
-          const SortEv xa = se[a], xb = se[b];
-          if (sortev_gt(xa, xb) == ((a & k) == 0)) {
-            se[a] = xb;
-            se[b] = xa;
-          }
-        }
-        __syncwarp();
-      }
-    }
+    bitonic_sort_shared(tau, key, val, n2, lane, 32, true);
     // sorted arrival times into the bucket's first half, weights into its second
     double *st = reinterpret_cast<double *>(ev);
     float *sv = reinterpret_cast<float *>(ev + cap / 2);
     for (uint32_t e = lane; e < n; e += 32) {
-      const SortEv x = se[e];
-      st[e] = x.tau;
-      sv[e] = x.val;
+      st[e] = tau[e];
+      sv[e] = val[e];
     }
     __syncwarp();
   }
@@ -1546,6 +1536,10 @@ struct dpsnn_engine {
   std::vector<float> fix_vals;
   std::vector<uint32_t> fix_keys, fix_bucket;
   uint32_t *h_pin = nullptr;          // pinned {flags, spike count} for per-step reads
+  // spike lists are read on their own stream as soon as the compaction of
+  // their step is done, while the rest of that step (and later ones) run
+  cudaStream_t read_stream = nullptr;
+  cudaEvent_t ev_slot[RING_SLOTS] = {};
 };
 
 static void collect_timings(dpsnn_engine *e);
@@ -2067,6 +2061,9 @@ extern "C" int dpsnn_create(const dpsnn_params *p, const dpsnn_options *opts, dp
     ok = cudaEventCreateWithFlags(&e->ev_bath[b], cudaEventDisableTiming) == cudaSuccess &&
          cudaEventCreateWithFlags(&e->ev_neuron[b], cudaEventDisableTiming) == cudaSuccess;
   ok = ok && cudaEventCreateWithFlags(&e->ev_start, cudaEventDisableTiming) == cudaSuccess;
+  ok = ok && cudaStreamCreateWithFlags(&e->read_stream, cudaStreamNonBlocking) == cudaSuccess;
+  for (int k = 0; k < RING_SLOTS && ok; k++)
+    ok = cudaEventCreateWithFlags(&e->ev_slot[k], cudaEventDisableTiming) == cudaSuccess;
   ok = ok && cudaMallocHost((void **)&e->h_pin, 2 * sizeof(uint32_t)) == cudaSuccess;
   if (!ok) {
     const int dev = e->device;
@@ -2095,6 +2092,12 @@ extern "C" void dpsnn_destroy(dpsnn_engine *e) {
     if (e->ev_neuron[b]) cudaEventDestroy(e->ev_neuron[b]);
   }
   if (e->ev_start) cudaEventDestroy(e->ev_start);
+  for (int k = 0; k < RING_SLOTS; k++)
+    if (e->ev_slot[k]) cudaEventDestroy(e->ev_slot[k]);
+  if (e->read_stream) {
+    cudaStreamSynchronize(e->read_stream);
+    cudaStreamDestroy(e->read_stream);
+  }
   if (e->h_pin) cudaFreeHost(e->h_pin);
   if (e->bath_stream) cudaStreamDestroy(e->bath_stream);
   if (e->stream) cudaStreamDestroy(e->stream);
@@ -2199,6 +2202,7 @@ static int enqueue_step(dpsnn_engine *e) {
   timed_launch_begin(e, 0);
   compact_kernel<<<e->grid_neuron, NEURON_BLOCK, 0, e->stream>>>(d);
   timed_launch_end(e, 0);
+  cudaEventRecord(e->ev_slot[t % RING_SLOTS], e->stream);   // slot t is final
   if (e->hnet.stdp_on) {
     timed_launch_begin(e, 4);
     causal_stdp_kernel<<<e->grid_deliver, 256, 0, e->stream>>>(d);
@@ -2270,20 +2274,25 @@ extern "C" int dpsnn_spikes(dpsnn_engine *e, uint32_t t_ms, uint32_t *ids, doubl
     return dpsnn_fail(DPSNN_E_STATE, "step %u is not among the last %d completed steps", t_ms, RING_SLOTS);
   cudaSetDevice(e->device);
   const uint32_t slot = t_ms % RING_SLOTS;
-  // one round trip for the error flags and the count, one for the list
-  CK(cudaMemcpyAsync(e->h_pin, e->d.flags, 4, cudaMemcpyDeviceToHost, e->stream));
-  CK(cudaMemcpyAsync(e->h_pin + 1, e->d.ring_cnt + slot, 4, cudaMemcpyDeviceToHost, e->stream));
-  CK(cudaStreamSynchronize(e->stream));
+  // wait only for the compaction of step t_ms (the rest of that step and
+  // later steps may still run): one round trip for the error flags and the
+  // count, one for the list
+  CK(cudaStreamWaitEvent(e->read_stream, e->ev_slot[slot], 0));
+  CK(cudaMemcpyAsync(e->h_pin, e->d.flags, 4, cudaMemcpyDeviceToHost, e->read_stream));
+  CK(cudaMemcpyAsync(e->h_pin + 1, e->d.ring_cnt + slot, 4, cudaMemcpyDeviceToHost, e->read_stream));
+  CK(cudaStreamSynchronize(e->read_stream));
   int rc = flags_error(e->h_pin[0]);
   if (rc) return rc;
   const uint32_t cnt = e->h_pin[1];
   *count = cnt;
   const uint32_t k = std::min(cnt, cap);
   if (k && ids)
-    CK(cudaMemcpyAsync(ids, e->d.ring_ids + (size_t)slot * e->hnet.N, 4ull * k, cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaMemcpyAsync(ids, e->d.ring_ids + (size_t)slot * e->hnet.N, 4ull * k, cudaMemcpyDeviceToHost,
+                       e->read_stream));
   if (k && te)
-    CK(cudaMemcpyAsync(te, e->d.ring_te + (size_t)slot * e->hnet.N, 8ull * k, cudaMemcpyDeviceToHost, e->stream));
-  if (k && (ids || te)) CK(cudaStreamSynchronize(e->stream));
+    CK(cudaMemcpyAsync(te, e->d.ring_te + (size_t)slot * e->hnet.N, 8ull * k, cudaMemcpyDeviceToHost,
+                       e->read_stream));
+  if (k && (ids || te)) CK(cudaStreamSynchronize(e->read_stream));
   return 0;
 }
 

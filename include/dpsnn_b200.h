@@ -121,7 +121,9 @@ uint64_t dpsnn_events_delivered(const dpsnn_engine *e);
 
 /* Spike list detected at step t_ms (one of the last 80 steps): ascending
  * neuron index, with emission times.  *count receives the number of spikes;
- * at most cap are written. */
+ * at most cap are written.  Waits only until that step's list is final (its
+ * compaction), so the rest of the step and any later queued steps keep
+ * running; reports device errors raised so far. */
 int dpsnn_spikes(dpsnn_engine *e, uint32_t t_ms, uint32_t *ids, double *te,
                  uint32_t cap, uint32_t *count);
 
