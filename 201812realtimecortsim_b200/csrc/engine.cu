@@ -866,35 +866,56 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d, uint32_t t) {
       }
       unsigned long long my_start = 0;
       uint32_t my_cnt = 0;
+      // One wait covers the whole chunk while every neuron takes the fast
+      // path (at most 2 * BATH_FAST_LANES draws each); after a fall-back the
+      // bound is checked per neuron again.
+      const unsigned long long base = pos;
+      uint32_t rel = 0;   // pos - base
+      bool safe = true;
+      uint32_t spins = 0;
+      while (lim < base + 64ull * BATH_FAST_LANES + BATH_WINDOW) {
+        if (vs.flag[rr % BATH_ROUNDS] == rr + 1) {
+          rr++;
+          lim = s.conv_base + (unsigned long long)rr * 24;
+          __threadfence_block();
+        } else if (++spins > BATH_SPIN_LIMIT) {
+          fail = true;
+          break;
+        }
+      }
+      if (fail) break;
       for (uint32_t j = 0; j < cn; j++) {
         const uint32_t lo = __shfl_sync(0xffffffffu, my_lo, j);
         const uint32_t hi1 = __shfl_sync(0xffffffffu, my_hi1, j);
         const uint32_t misc = __shfl_sync(0xffffffffu, my_misc, j);
-        uint32_t spins = 0;
-        while (lim < pos + BATH_WINDOW) {
-          if (vs.flag[rr % BATH_ROUNDS] == rr + 1) {
-            rr++;
-            lim = s.conv_base + (unsigned long long)rr * 24;
-            __threadfence_block();
-          } else if (++spins > BATH_SPIN_LIMIT) {
-            fail = true;
-            break;
+        if (!safe) {
+          while (lim < base + rel + BATH_WINDOW) {
+            if (vs.flag[rr % BATH_ROUNDS] == rr + 1) {
+              rr++;
+              lim = s.conv_base + (unsigned long long)rr * 24;
+              __threadfence_block();
+            } else if (++spins > BATH_SPIN_LIMIT) {
+              fail = true;
+              break;
+            }
           }
+          if (fail) break;
         }
-        if (fail) break;
-        const unsigned long long start = pos;
+        const uint32_t start_rel = rel;
         uint32_t c = 0;
         if (misc) {
           // lane L: the lapses at pos+1, pos+3, .., pos+1+2L, in 2^-20 units
-          const uint32_t p32 = (uint32_t)pos;
+          const uint32_t p32 = (uint32_t)base + rel;
           const uint32_t F = s.q[(p32 + 1 + 2 * lane) & M] - s.q[(p32 - 1) & M];
-          // F grows with L, so the lanes below the bounds are a prefix of m lanes
-          const uint32_t m = __reduce_add_sync(0xffffffffu, F < lo ? 1u : 0u);
+          const uint32_t below = __ballot_sync(0xffffffffu, F < lo);
           const uint32_t above = __ballot_sync(0xffffffffu, F >= hi1);
+          const uint32_t m = __popc(below);   // F grows with L: below is a prefix
           if (m < (misc & 0xFFu) && ((above >> m) & 1u)) {
             c = m + 1;
-            pos += 2ull * c;
+            rel += 2 * c;
           } else {
+            safe = false;
+            pos = base + rel;
             // the reference's loop (regularDynamicTimeStep :604-640)
             double nbv = __shfl_sync(0xffffffffu, my_nb, j);
             const double inv = __shfl_sync(0xffffffffu, my_inv, j);
@@ -935,14 +956,16 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d, uint32_t t) {
                 pos += 1;
               } while (nbv < T1);
             }
+            rel = (uint32_t)(pos - base);
           }
         }
         if (fail) break;
         if (lane == j) {
-          my_start = start;
+          my_start = base + start_rel;
           my_cnt = c;
         }
       }
+      pos = base + rel;
       if (fail) break;
       // parallel emission of the chunk's events
       uint32_t incl = my_cnt;
