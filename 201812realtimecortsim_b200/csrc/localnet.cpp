@@ -183,6 +183,12 @@ void localNetProcess_init(DALProcess *p) {
   }
   LocalNet *n = new LocalNet();
   if (dpsnn_params_from_env(nullptr, &n->par)) die("getParameters");
+  // side outputs of the reference that this process does not write
+  for (const char *v : {"env_statSTDPevent_writeDisable", "env_statSynPeriodicProbe_writeDisable"}) {
+    const char *s = getenv(v);
+    if (s && atoi(s) == 0)
+      fprintf(stderr, "WARNING %s=0: those statistics files are not written by this engine\n", v);
+  }
   dpsnn_options opt;
   memset(&opt, 0, sizeof opt);
   opt.device = (int)env_u32_or("DPSNN_DEVICE", 0);
