@@ -100,6 +100,7 @@ struct NetConst {
   float causal_tab[128], anti_tab[128];
   float stdp_drift, stdp_tauDecay;
   uint32_t ev_cap, ovf_cap;
+  uint32_t light_max;   // neurons with more synaptic events take the heavy path
   uint32_t bath_need;  // largest maxExternCurrentCount
   uint32_t delay_exp;  // getRandomDelay_EXP instead of _UNI
   float inv_log_tn;    // (float)(1.0 / log(0.05)), the EXP tail constant
@@ -1168,7 +1169,7 @@ __global__ void __launch_bounds__(NEURON_BLOCK) neuron_kernel(Dev d) {
   if (i < N) {
     const uint32_t cnt = d.ev_cnt[i];
     d.ev_cnt[i] = 0;
-    if (cnt > LOCAL_EVENTS) {
+    if (cnt > net->light_max) {
       const uint32_t path = (cnt <= warp_path_max(net)) ? 0u : 1u;
       const uint32_t k = atomicAdd(&d.heavy_cnt[path], 1u);
       if (k < N) {
@@ -1277,15 +1278,25 @@ __global__ void __launch_bounds__(HEAVY_SORT_WARPS * 32) heavy_sort_kernel(Dev d
     uint2 *ev = d.ev + (size_t)i * cap;
     uint32_t n2 = 1;
     while (n2 < n) n2 <<= 1;
-    for (uint32_t e = lane; e < n2; e += 32) {
-      if (e < n) {
-        const uint2 x = ev[e];
-        key[e] = x.x;
-        val[e] = __uint_as_float(x.y);
-        tau[e] = event_time(d, x.x, t, D, N);
-      } else {
-        tau[e] = INFINITY;
-        key[e] = 0xFFFFFFFFu;
+    // the bucket's events and their arrival times, 4 per lane in flight
+    for (uint32_t e0 = 0; e0 < n2; e0 += 128) {
+      uint2 x[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const uint32_t e = e0 + 32 * u + lane;
+        if (e < n) x[u] = ev[e];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const uint32_t e = e0 + 32 * u + lane;
+        if (e < n) {
+          key[e] = x[u].x;
+          val[e] = __uint_as_float(x[u].y);
+          tau[e] = event_time(d, x[u].x, t, D, N);
+        } else if (e < n2) {
+          tau[e] = INFINITY;
+          key[e] = 0xFFFFFFFFu;
+        }
       }
     }
     __syncwarp();
@@ -1759,6 +1770,11 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
   n.stdp_drift = p->stdp_drift;
   n.stdp_tauDecay = p->stdp_tauDecay_s;
   n.ev_cap = (o && o->events_per_neuron) ? o->events_per_neuron : DEFAULT_EVENT_CAP;
+  {  // tuning knob: the largest event count of the thread-per-neuron path
+    const char *lm = getenv("DPSNN_LIGHT_EVENTS");
+    n.light_max = lm ? (uint32_t)atoi(lm) : LOCAL_EVENTS;
+    if (n.light_max < 1 || n.light_max > LOCAL_EVENTS) n.light_max = LOCAL_EVENTS;
+  }
   if (n.ev_cap > 4096) n.ev_cap = 4096;
   if (!(o && o->events_per_neuron)) {   // default: at most 16 GiB of event slots
     while (n.ev_cap > 64 && 8ull * n.ev_cap * n.N > (16ull << 30)) n.ev_cap >>= 1;

@@ -88,8 +88,9 @@ typedef struct {
 
 /* Engine capacities (0 = default). */
 typedef struct {
-  uint32_t events_per_neuron;     /* synaptic events per neuron per step kept
-                                     in the fast path (default 64) */
+  uint32_t events_per_neuron;     /* per-target event slots per step (default
+                                     1024, halved while they would exceed
+                                     16 GiB; at most 4096) */
   uint32_t overflow_events;       /* events beyond that, per step (default 1<<22) */
   int device;                     /* CUDA device ordinal (default current) */
 } dpsnn_options;
