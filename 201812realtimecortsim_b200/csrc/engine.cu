@@ -621,10 +621,12 @@ __global__ void __launch_bounds__(DELIVER_THREADS) deliver_kernel(Dev d) {
 // rank runs a shared-memory pipeline:
 //   warp 1     extends the lagged Fibonacci sequence 24 values per round
 //              (x[n] = x[n-55] - x[n-24] mod 1e9) into a ring of raw draws;
-//   warps 2..7 convert each round into the LUT index (uint32)(u*256) and the
+//   warps 2,3,5,6,7 convert each round into the LUT index (uint32)(u*256) and the
 //              lapse factor -logf((float)(1-u)), and extend q[], the running
 //              sum over draws of one parity of the lapses in 2^-20 units
 //              (q[n] = q[n-2] + round(lap[n] * 2^20), integers mod 2^32);
+//   warp 4     stays idle: warps go to the SM's four schedulers by index, so
+//              this leaves warp 0 a scheduler of its own;
 //   warp 0     walks the neurons.  The number of events c of a neuron is the
 //              first c at which nextBath + sum of c lapses * invNuExt reaches
 //              t+1.  Per chunk of 32 neurons each lane turns its neuron's
@@ -646,6 +648,7 @@ __global__ void __launch_bounds__(DELIVER_THREADS) deliver_kernel(Dev d) {
 #define BATH_MAX_EXT 2048      // largest maxExternCurrentCount supported
 #define BATH_SPIN_LIMIT (1u << 26)
 #define BATH_FAST_LANES 32     // events decided by one ballot
+#define BATH_IDLE_WARP 4       // shares the consumer's scheduler: left idle
 #define BATH_WINDOW (2 * BATH_FAST_LANES + 2)   // draws a ballot reads past pos
 
 struct BathSmem {
@@ -768,7 +771,7 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d, uint32_t t) {
       if (lane == 0) vs.raw_end = n0 + 24;
       r++;
     }
-  } else if (warp >= 2) {
+  } else if (warp >= 2 && warp != BATH_IDLE_WARP) {
     // ---- converters: rounds are claimed in order and published in order
     while (true) {
       uint32_t r = 0;
@@ -819,7 +822,7 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d, uint32_t t) {
         vs.published = r + 1;
       }
     }
-  } else {
+  } else if (warp == 0) {
     // ---- consumer (warp 0)
     unsigned long long pos = s.pos;
     unsigned long long lim = s.raw_end;   // converted draws available (prefix)
@@ -885,6 +888,7 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d, uint32_t t) {
         }
       }
       if (fail) break;
+#pragma unroll 2
       for (uint32_t j = 0; j < cn; j++) {
         const uint32_t lo = __shfl_sync(0xffffffffu, my_lo, j);
         const uint32_t hi1 = __shfl_sync(0xffffffffu, my_hi1, j);
