@@ -38,7 +38,7 @@
 #define MBIG 1000000000
 #define MSEED 161803398
 #define NEURON_BLOCK 256
-#define LOCAL_EVENTS 32        // per-thread event buffer of the neuron kernel
+#define LOCAL_EVENTS 16        // per-thread event buffer of the neuron kernel
 #define NEURON_BATCH 8         // event loads in flight per thread
 #define DEFAULT_EVENT_CAP 1024 // per-target event slots per step (capped by memory)
 
