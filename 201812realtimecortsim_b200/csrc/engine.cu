@@ -510,7 +510,7 @@ __global__ void causal_stdp_kernel(Dev d) {
 // them (delay descending, then source ascending), which breaks ties between
 // equal arrival times.
 #define DELIVER_THREADS 256
-#define DELIVER_UNROLL 8
+#define DELIVER_UNROLL 4
 
 __device__ static inline void deliver_event(const Dev &d, const NetConst *net, uint64_t k, uint32_t key,
                                             uint32_t t, bool stdp, uint32_t cap, uint32_t j, float wf) {
