@@ -139,7 +139,8 @@ DD_HD double log_cr(double x) {
 
 // Fix-up table of the C library's logf on (0,1]: sorted input bit patterns
 // keys[] with the library's results vals[]; bucket[b] is the first entry
-// whose key>>12 is >= b + LOGF_FIX_BASE.
+// whose key>>12 is >= b + LOGF_FIX_BASE (kept in the file; the engine finds a
+// key through a one-bit-per-float filter and a binary search of keys[]).
 #define LOGF_FIX_BASE (0x30000000u >> 12)
 #define LOGF_FIX_NBUCKET ((0x3F800000u >> 12) - LOGF_FIX_BASE + 2)
 typedef struct {
@@ -156,15 +157,4 @@ DD_HD float logf_cr_from(float x, double y_approx) {
   float f2 = (float)(y_approx * (1.0 - 0x1p-49));
   if (f1 == f2) return f1;
   return (float)log_cr((double)x);
-}
-
-DD_HD float logf_fixup_lookup(logf_fixup_t fx, float x, float fallback) {
-  union { float f; uint32_t u; } b;
-  b.f = x;
-  uint32_t key = b.u;
-  if (key < 0x30000000u || key > 0x3F800000u || fx.n == 0) return fallback;
-  uint32_t bk = (key >> 12) - LOGF_FIX_BASE;
-  for (uint32_t i = fx.bucket[bk]; i < fx.bucket[bk + 1]; i++)
-    if (fx.keys[i] == key) return fx.vals[i];
-  return fallback;
 }

@@ -1264,17 +1264,19 @@ __device__ static inline uint32_t warp_path_max(const NetConst *net) {
   return min(net->ev_cap / 2, (uint32_t)HEAVY_WARP_MAX);
 }
 
+// The warp sort keeps times (8 B) and {key, weight} pairs (8 B, key in the
+// high half) in two shared arrays: a compare-exchange is four 8-byte loads
+// and at most four 8-byte stores (the kernel is bound by shared-memory
+// issue); equal times order by key, unique per target.
 __global__ void __launch_bounds__(HEAVY_SORT_WARPS * 32) heavy_sort_kernel(Dev d) {
   extern __shared__ __align__(16) unsigned char hs_raw[];
   const NetConst *net = d.net;
   const uint32_t t = *d.t, N = net->N, D = net->D, cap = net->ev_cap, wmax = warp_path_max(net);
   const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  double *tau_base = reinterpret_cast<double *>(hs_raw);
-  uint32_t *key_base = reinterpret_cast<uint32_t *>(tau_base + HEAVY_SORT_WARPS * HEAVY_WARP_MAX);
-  float *val_base = reinterpret_cast<float *>(key_base + HEAVY_SORT_WARPS * HEAVY_WARP_MAX);
-  double *tau = tau_base + (size_t)w * HEAVY_WARP_MAX;
-  uint32_t *key = key_base + (size_t)w * HEAVY_WARP_MAX;
-  float *val = val_base + (size_t)w * HEAVY_WARP_MAX;
+  double *tau = reinterpret_cast<double *>(hs_raw) + (size_t)w * HEAVY_WARP_MAX;
+  unsigned long long *kv =
+      reinterpret_cast<unsigned long long *>(hs_raw + (size_t)HEAVY_SORT_WARPS * HEAVY_WARP_MAX * 8) +
+      (size_t)w * HEAVY_WARP_MAX;
   const uint32_t nh = min(d.heavy_cnt[0], N);
   for (uint32_t hh = blockIdx.x * HEAVY_SORT_WARPS + w; hh < nh; hh += gridDim.x * HEAVY_SORT_WARPS) {
     const uint32_t i = d.heavy_list[hh], n = d.heavy_list[N + hh];
@@ -1294,23 +1296,39 @@ __global__ void __launch_bounds__(HEAVY_SORT_WARPS * 32) heavy_sort_kernel(Dev d
       for (int u = 0; u < 4; u++) {
         const uint32_t e = e0 + 32 * u + lane;
         if (e < n) {
-          key[e] = x[u].x;
-          val[e] = __uint_as_float(x[u].y);
           tau[e] = event_time(d, x[u].x, t, D, N);
+          kv[e] = ((unsigned long long)x[u].x << 32) | x[u].y;
         } else if (e < n2) {
           tau[e] = INFINITY;
-          key[e] = 0xFFFFFFFFu;
+          kv[e] = ~0ull;
         }
       }
     }
     __syncwarp();
-    bitonic_sort_shared(tau, key, val, n2, lane, 32, true);
+    for (uint32_t k = 2; k <= n2; k <<= 1) {
+      for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+        // pair p compares a = p with bit j inserted as 0, and b = a | j
+        for (uint32_t p = lane; p < (n2 >> 1); p += 32) {
+          const uint32_t a = ((p & ~(j - 1)) << 1) | (p & (j - 1)), b = a | j;
+          const double ta = tau[a], tb = tau[b];
+          const unsigned long long ka = kv[a], kb = kv[b];
+          const bool gt = (ta > tb) || (ta == tb && ka > kb);
+          if (gt == ((a & k) == 0)) {
+            tau[a] = tb;
+            tau[b] = ta;
+            kv[a] = kb;
+            kv[b] = ka;
+          }
+        }
+        __syncwarp();
+      }
+    }
     // sorted arrival times into the bucket's first half, weights into its second
     double *st = reinterpret_cast<double *>(ev);
     float *sv = reinterpret_cast<float *>(ev + cap / 2);
     for (uint32_t e = lane; e < n; e += 32) {
       st[e] = tau[e];
-      sv[e] = val[e];
+      sv[e] = __uint_as_float((uint32_t)kv[e]);
     }
     __syncwarp();
   }
