@@ -512,9 +512,11 @@ __global__ void causal_stdp_kernel(Dev d) {
 #define DELIVER_THREADS 256
 #define DELIVER_UNROLL 4
 
+// Stores one event in slot s of target j's list (taken by the caller's
+// atomicAdd on ev_cnt[j]), or in the overflow list past the bucket.
 __device__ static inline void deliver_event(const Dev &d, const NetConst *net, uint64_t k, uint32_t key,
-                                            uint32_t t, bool stdp, uint32_t cap, uint32_t j, float wf) {
-  const uint32_t s = atomicAdd(&d.ev_cnt[j], 1u);
+                                            uint32_t t, bool stdp, uint32_t cap, uint32_t j, float wf,
+                                            uint32_t s) {
   if (s < cap) {
     d.ev[(size_t)j * cap + s] = make_uint2(key, __float_as_uint(wf));
   } else {
@@ -604,9 +606,14 @@ __global__ void __launch_bounds__(DELIVER_THREADS) deliver_kernel(Dev d) {
           wf[u] = ((float)__ldg(&d.w16[k[u]])) * w2f;
         }
       }
+      // all slot atomics in flight before the dependent stores
+      uint32_t sl[DELIVER_UNROLL];
 #pragma unroll
       for (int u = 0; u < DELIVER_UNROLL; u++)
-        if (kk[u] != 0xFFFFFFFFu) deliver_event(d, net, k[u], kk[u], t, stdp, cap, jj[u], wf[u]);
+        if (kk[u] != 0xFFFFFFFFu) sl[u] = atomicAdd(&d.ev_cnt[jj[u]], 1u);
+#pragma unroll
+      for (int u = 0; u < DELIVER_UNROLL; u++)
+        if (kk[u] != 0xFFFFFFFFu) deliver_event(d, net, k[u], kk[u], t, stdp, cap, jj[u], wf[u], sl[u]);
     }
     __syncwarp();
   }
