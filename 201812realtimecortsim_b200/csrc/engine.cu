@@ -534,7 +534,7 @@ __device__ static inline void deliver_event(const Dev &d, const NetConst *net, u
   }
 }
 
-__global__ void __launch_bounds__(DELIVER_THREADS, 5) deliver_kernel(Dev d) {
+__global__ void __launch_bounds__(DELIVER_THREADS) deliver_kernel(Dev d) {
   const NetConst *net = d.net;
   const uint32_t t = *d.t, N = net->N, D = net->D, cap = net->ev_cap;
   __shared__ uint32_t s_pre[RING_SLOTS + 1];
