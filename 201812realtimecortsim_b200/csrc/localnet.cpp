@@ -167,6 +167,72 @@ void write_chrono_window(const LocalNet &n, uint32_t h) {
   fclose(f);
 }
 
+// The Perseo .ini description of each rank's modules (writeIniFiles,
+// DPSNN_writeIniFiles.c:31-158; the reference compiles the call out of its
+// stock build, DPSNN_localNet_init.c:245-247): PerseoConFile_h<h>.txt with one
+// line per (source population, target population, stencil cell) of non-zero
+// connection probability, PerseoModFile_h<h>.txt with one line per local
+// sub-population.  Connection probabilities mirror the explicit stencil
+// (DPSNN_LIFCAconnectome.cpp); the bath efficacy is generateSourceNeuCExt
+// (:871-887).
+void write_ini_files(const LocalNet &n) {
+  const dpsnn_params &p = n.par;
+  const uint32_t S = p.stencil_dim, st = 2 * S - 1, M = S - 1, nsub = p.nsub;
+  if (floorf(n.locCFT) != n.locCFT) return;
+  const uint32_t lcft = (uint32_t)floorf(n.locCFT);
+  auto prob = [&](uint32_t s, uint32_t t, uint32_t x, uint32_t y) -> float {
+    const uint32_t dx = x >= M ? x - M : M - x, dy = y >= M ? y - M : M - y;
+    return p.spec[((size_t)(s * nsub + t) * S + dx) * S + dy];
+  };
+  for (uint32_t h = 0; h < n.P; h++) {
+    char fc[40], fm[40];
+    snprintf(fc, sizeof fc, "PerseoConFile_h%u.txt", h);
+    snprintf(fm, sizeof fm, "PerseoModFile_h%u.txt", h);
+    FILE *fpc = fopen(fc, "w"), *fpm = fopen(fm, "w");
+    if (!fpc || !fpm) {
+      printf("ERROR NULL fp\n");
+      fflush(stdout);
+      exit(0);
+    }
+    const uint32_t first = h * n.locN, last = first + n.locN - 1;
+    const uint32_t fx = (first / n.npcm) % p.cfx, fy = (first / n.npcm) / p.cfx;
+    const uint32_t lx = (last / n.npcm) % p.cfx, ly = (last / n.npcm) / p.cfx;
+    for (uint32_t cx = fx; cx <= lx; cx++)
+      for (uint32_t cy = fy; cy <= ly; cy++) {
+        const uint32_t this_cf = cx + cy * p.cfx, loc_cf = this_cf % lcft;
+        const uint32_t src_cf = loc_cf + lcft * h;
+        for (uint32_t sx = 0; sx < st; sx++)
+          for (uint32_t sy = 0; sy < st; sy++) {
+            const int32_t tx = (int32_t)cx + (int32_t)sx - (int32_t)M, ty = (int32_t)cy + (int32_t)sy - (int32_t)M;
+            if (tx < 0 || tx >= (int32_t)p.cfx || ty < 0 || ty >= (int32_t)p.cfy) continue;
+            const uint32_t tgt_cf = (uint32_t)tx + p.cfx * (uint32_t)ty;
+            for (uint32_t tp = 0; tp < nsub; tp++)
+              for (uint32_t sp = 0; sp < nsub; sp++) {
+                const float cp = prob(sp, tp, sx, sy);
+                const double dmin = (double)p.DMin[sp * nsub + tp] + 0.5, dmax = (double)p.DMax[sp * nsub + tp] + 0.5;
+                if (cp > 0.0)
+                  fprintf(fpc, " %5d %5d     %g   %g   %g   '%s'   %8g   %g\n", (int)(nsub * tgt_cf + tp),
+                          (int)(nsub * src_cf + sp), (double)cp, dmin, dmax, "Fixed",
+                          (double)p.J[sp * nsub + tp], (double)p.DJ[sp * nsub + tp]);
+              }
+          }
+        uint32_t bx = cx, by = cy;   // generateSourceNeuCExt: mirrored, clamped
+        if (bx >= p.cfx / 2) bx = p.cfx - 1 - bx;
+        if (by >= p.cfy / 2) by = p.cfy - 1 - by;
+        if (bx >= S) bx = S - 1;
+        if (by >= S) by = S - 1;
+        const float cext = (float)p.bath[bx * S + by];
+        for (uint32_t sp = 0; sp < nsub; sp++)
+          fprintf(fpm, " %6d   %g   %g   %g   %7g   %g   %g   %g   %g   %g   %4g   %4g   %d \n", (int)p.count[sp],
+                  (double)p.JExt[sp], (double)p.DJExt[sp], (double)cext, (double)p.NuExt[sp], (double)p.Tau[sp],
+                  (double)p.Theta[sp], (double)p.H[sp], (double)p.Tarp[sp], (double)p.AlphaC[sp],
+                  (double)p.TauC[sp], (double)p.gC[sp], 0);
+      }
+    fclose(fpc);
+    fclose(fpm);
+  }
+}
+
 uint32_t env_u32_or(const char *name, uint32_t dflt) {
   const char *s = getenv(name);
   return s ? (uint32_t)atoi(s) : dflt;
@@ -189,17 +255,18 @@ void localNetProcess_init(DALProcess *p) {
     if (s && atoi(s) == 0)
       fprintf(stderr, "WARNING %s=0: those statistics files are not written by this engine\n", v);
   }
-  dpsnn_options opt;
-  memset(&opt, 0, sizeof opt);
-  opt.device = (int)env_u32_or("DPSNN_DEVICE", 0);
-  if (dpsnn_create(&n->par, &opt, &n->eng)) die("localNetClass::init");
   const dpsnn_params &q = n->par;
   n->P = q.glob_h;
   n->globCFT = q.cfx * q.cfy;
   n->npcm = 0;
   for (uint32_t s = 0; s < q.nsub; s++) n->npcm += q.count[s];
-  n->locN = dpsnn_glob_n(n->eng) / n->P;
+  n->locN = n->npcm * n->globCFT / n->P;
   n->locCFT = ((float)n->globCFT / (float)n->P);
+  if (env_u32_or("DPSNN_WRITE_INI_FILES", 0) == 1) write_ini_files(*n);
+  dpsnn_options opt;
+  memset(&opt, 0, sizeof opt);
+  opt.device = (int)env_u32_or("DPSNN_DEVICE", 0);
+  if (dpsnn_create(&n->par, &opt, &n->eng)) die("localNetClass::init");
   n->max_ms = (int32_t)q.total_sim_time_ms;
   n->chrono = env_u32_or("env_chrono", 0);
   n->chrono_start = env_u32_or("env_startPartialChrono_ms", 0);

@@ -44,6 +44,8 @@ REF_MP = os.path.join(ROOT, "oracle", "_ref", "dpsnn_ref_mp")
 # built without -DDelayUniform: the reference Makefile's exponential delays
 REF_EXP_HP = os.path.join(ROOT, "oracle", "_ref", "dpsnn_ref_exp_hp")
 REF_EXP = os.path.join(ROOT, "oracle", "_ref", "dpsnn_ref_exp")
+# the Perseo .ini writer switched on (compiled out of the stock build)
+REF_INI = os.path.join(ROOT, "oracle", "_ref", "dpsnn_ref_ini")
 KAT = os.path.join(ROOT, "oracle", "_ref", "ref_kat")
 
 
@@ -74,7 +76,7 @@ def run(binary, cfg, workdir):
 
 
 def main():
-    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", "kat", "mp", "exp"], check=True,
+    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", "kat", "mp", "exp", "ini"], check=True,
                    capture_output=True)
     with open(os.path.join(HERE, "ref_kat.txt"), "w") as f:
         f.write(subprocess.run([KAT], check=True, capture_output=True, text=True).stdout)
@@ -109,6 +111,13 @@ def main():
                 for h in range(cfg.glob_h):
                     with open(os.path.join(std, f"spikes-sec0-C{cfg.n_modules}-H{cfg.glob_h}-h{h:03d}.dat")) as g:
                         f.write(g.read())
+            if cfg.glob_h == 1 and not cfg.delay_exponential:
+                ini = os.path.join(td, "ini")
+                short = make()
+                short.total_ms = 10   # the files are written at init
+                run(REF_INI, short, ini)
+                entry["ini_sha256"] = {fn: sha256(os.path.join(ini, fn)) for fn in sorted(os.listdir(ini))
+                                       if fn.startswith(("PerseoConFile_", "PerseoModFile_"))}
         # synaptic events delivered in the run (identical dynamics in the
         # restatement, pinned by the raster and dump checks)
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
