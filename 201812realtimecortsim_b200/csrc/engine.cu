@@ -402,6 +402,15 @@ struct Dev {
   int16_t *w16;
   float *tderiv;
   int32_t *last_act;
+  // LTP probe (null unless enabled): weight and trace before the update,
+  // and the trace after it before its decay
+  int16_t *probe_w;
+  float *probe_td, *probe_td_mid;
+  // STDP event log of one step (null unless enabled): {synapse index lo/hi,
+  // post | anti-causal << 31, contribution bits} of rank 0's synapses from
+  // rank-0 neurons with a non-zero contribution
+  uint4 *stdp_log;
+  uint32_t *stdp_log_cnt;
   uint64_t *in_ptr;
   uint32_t *in_idx;
   // ring
@@ -477,6 +486,36 @@ __global__ void compact_kernel(Dev d) {
   }
 }
 
+#define STDP_LOG_CAP DPSNN_STDP_LOG_CAP   // STDP event records per step
+
+// One record of the STDP event log (the statSTDPevent.write calls of
+// DPSNN_neuron_sim.c:152-166 and :230-246, which report rank 0's synapses
+// whose both ends are rank-0 neurons); the host restores the reference's order.
+__device__ static inline void stdp_log_append(const Dev &d, uint64_t k, uint32_t post, uint32_t anti, float c) {
+  const uint32_t o = atomicAdd(d.stdp_log_cnt, 1u);
+  if (o < STDP_LOG_CAP)
+    d.stdp_log[o] = make_uint4((uint32_t)k, (uint32_t)(k >> 32), post | (anti << 31), __float_as_uint(c));
+  else
+    atomicOr(d.flags, F_OVERFLOW);
+}
+
+// The anti-causal records of the STDP event log, after delivery: a synapse
+// delivered at step t carries last_act == t (one delivery per synapse and
+// step, none at step 0), and its contribution is the one delivery added.
+__global__ void stdp_anti_log_kernel(Dev d) {
+  const NetConst *net = d.net;
+  const uint32_t t = *d.t;
+  if (t == 0 || !(t >= net->start_pl && t <= net->stop_pl)) return;
+  const uint64_t end = d.row_ptr[net->locN];
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < end; k += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t j = d.post[k];
+    if (j >= net->locN || d.last_act[k] != (int32_t)t) continue;
+    const int td = (int)t - d.last_spike_ms[j];
+    const float a = (td < 128) ? net->anti_tab[td] : 0.0f;
+    if (a != 0.0f) stdp_log_append(d, k, j, 1u, a);
+  }
+}
+
 // Causal STDP at detection (causalSTDP_ms_ofBackwardSynapses,
 // DPSNN_neuron_sim.c:94-177): one warp per spiking neuron walks its incoming
 // synapses.
@@ -495,6 +534,8 @@ __global__ void causal_stdp_kernel(Dev d) {
       int td = (int)t - 1 - la;
       float fc = (la != 0 && td < 128) ? net->causal_tab[td] : 0.0f;
       d.tderiv[s] = d.tderiv[s] + fc;
+      if (d.stdp_log && fc != 0.0f && t != 0 && i < net->locN && s < d.row_ptr[net->locN])
+        stdp_log_append(d, s, i, 0u, fc);
     }
   }
 }
@@ -1480,8 +1521,13 @@ __global__ void ltp_kernel(Dev d) {
       float rmaxv = (float)(2.0 * net->J[tp * DPSNN_MAX_SUBPOP + sp]);
       float clamp = 0.0f;
       float td = d.tderiv[k];
+      const int16_t w0 = d.w16[k];
+      if (d.probe_w) {
+        d.probe_w[k] = w0;
+        d.probe_td[k] = td;
+      }
       if (maxv > 0.0 && rmaxv > 0.0) {
-        float wF = (float)(d.w16[k] * net->w2f);
+        float wF = (float)(w0 * net->w2f);
         float dF = td;
         dF += net->stdp_drift;
         wF = wF + dF;
@@ -1490,6 +1536,7 @@ __global__ void ltp_kernel(Dev d) {
         d.w16[k] = (int16_t)(wF * net->f2w);
         td = dF;
       }
+      if (d.probe_w) d.probe_td_mid[k] = td;
       if (net->stdp_tauDecay == 1.0f)
         td = 0.0f;
       else
@@ -1587,6 +1634,10 @@ struct dpsnn_engine {
   int device = 0;
   uint64_t S = 0;
   uint32_t t_host = 0;   // steps enqueued
+  uint32_t probe_t = UINT32_MAX;   // step of the last LTP probe taken
+  uint32_t stdp_log_t = UINT32_MAX;   // step the STDP event log holds
+  std::vector<uint64_t> h_row;     // host copies of the CSR row and delay offsets
+  std::vector<uint16_t> h_so;      // (for the STDP event log's order)
   std::vector<void *> allocs;
   uint32_t grid_neuron = 0, grid_deliver = 0, grid_heavy = 0, grid_heavy_run = 0, grid_huge = 0;
   int timing = 0;
@@ -2262,6 +2313,10 @@ static int enqueue_step(dpsnn_engine *e) {
     e->bath_primed = true;
   }
   enqueue_bath(e, t + 1);
+  if (e->d.stdp_log) {
+    cudaMemsetAsync(e->d.stdp_log_cnt, 0, 4, e->stream);
+    e->stdp_log_t = t;
+  }
   Dev d = e->d;
   d.bath_time = e->bath_time2[b];
   d.bath_lut = e->bath_lut2[b];
@@ -2279,6 +2334,10 @@ static int enqueue_step(dpsnn_engine *e) {
   timed_launch_begin(e, 1);
   deliver_kernel<<<e->grid_deliver, DELIVER_THREADS, 0, e->stream>>>(d);
   timed_launch_end(e, 1);
+  if (d.stdp_log) {
+    stdp_anti_log_kernel<<<e->grid_deliver, 256, 0, e->stream>>>(d);
+    e->launches++;
+  }
   cudaStreamWaitEvent(e->stream, e->ev_bath[b], 0);
   timed_launch_begin(e, 3);
   neuron_kernel<<<e->grid_neuron, NEURON_BLOCK, 0, e->stream>>>(d);
@@ -2294,6 +2353,7 @@ static int enqueue_step(dpsnn_engine *e) {
   timed_launch_end(e, 7);
   cudaEventRecord(e->ev_neuron[b], e->stream);
   if (e->hnet.stdp_on) {
+    if (d.probe_w && t % 1000 == 999 && t >= e->hnet.start_pl && t <= e->hnet.stop_pl) e->probe_t = t;
     timed_launch_begin(e, 4);
     ltp_kernel<<<e->grid_deliver, 256, 0, e->stream>>>(d);
     timed_launch_end(e, 4);
@@ -2452,6 +2512,123 @@ extern "C" int dpsnn_backward_synapses(dpsnn_engine *e, uint32_t h, uint32_t *pr
         o++;
       }
     }
+  return 0;
+}
+
+extern "C" int dpsnn_enable_ltp_probe(dpsnn_engine *e) {
+  if (!e) return dpsnn_fail(DPSNN_E_PARAM, "null engine");
+  if (!e->hnet.stdp_on) return dpsnn_fail(DPSNN_E_PARAM, "the LTP probe needs plasticity switched on");
+  if (e->d.probe_w) return 0;
+  if (e->t_host) return dpsnn_fail(DPSNN_E_PARAM, "the LTP probe is enabled before the first step");
+  cudaSetDevice(e->device);
+  DALLOC(e->d.probe_w, e->S);
+  DALLOC(e->d.probe_td, e->S);
+  DALLOC(e->d.probe_td_mid, e->S);
+  return 0;
+}
+
+extern "C" int dpsnn_ltp_probe(dpsnn_engine *e, uint32_t h, uint32_t *t_ms, int16_t *w_before, float *td_before,
+                               int16_t *w_after, float *td_after) {
+  if (!e) return dpsnn_fail(DPSNN_E_PARAM, "null engine");
+  if (h >= e->hnet.P) return dpsnn_fail(DPSNN_E_PARAM, "rank %u out of range", h);
+  if (!e->d.probe_w) return dpsnn_fail(DPSNN_E_PARAM, "the LTP probe is not enabled");
+  if (e->probe_t == UINT32_MAX) return dpsnn_fail(DPSNN_E_PARAM, "no plasticity update has run yet");
+  HostCsr c;
+  int rc = fetch_csr(e, c, false);   // synchronises: the probe and the weights are final
+  if (rc) return rc;
+  std::vector<int16_t> pw(e->S);
+  std::vector<float> pt(e->S), pm(e->S);
+  CK(cudaMemcpy(pw.data(), e->d.probe_w, 2ull * e->S, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(pt.data(), e->d.probe_td, 4ull * e->S, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(pm.data(), e->d.probe_td_mid, 4ull * e->S, cudaMemcpyDeviceToHost));
+  if (t_ms) *t_ms = e->probe_t;
+  // the order of dpsnn_backward_synapses; the weights change only at an LTP
+  // update, so the live weights are those the last update wrote
+  const uint32_t N = e->hnet.N, D = e->hnet.D, locN = e->hnet.locN;
+  uint64_t o = 0;
+  for (uint32_t dl = 0; dl < D; dl++)
+    for (uint32_t P = 0; P < N; P++) {
+      uint64_t b = c.row[P] + c.so[(size_t)P * (D + 1) + dl], en = c.row[P] + c.so[(size_t)P * (D + 1) + dl + 1];
+      for (uint64_t k = b; k < en; k++) {
+        if (c.post[k] / locN != h) continue;
+        if (w_before) w_before[o] = pw[k];
+        if (td_before) td_before[o] = pt[k];
+        if (w_after) w_after[o] = c.w[k];
+        if (td_after) td_after[o] = pm[k];
+        o++;
+      }
+    }
+  return 0;
+}
+
+extern "C" int dpsnn_enable_stdp_events(dpsnn_engine *e) {
+  if (!e) return dpsnn_fail(DPSNN_E_PARAM, "null engine");
+  if (!e->hnet.stdp_on) return dpsnn_fail(DPSNN_E_PARAM, "the STDP event log needs plasticity switched on");
+  if (e->d.stdp_log) return 0;
+  if (e->t_host) return dpsnn_fail(DPSNN_E_PARAM, "the STDP event log is enabled before the first step");
+  cudaSetDevice(e->device);
+  HostCsr c;
+  int rc = fetch_csr(e, c, false);
+  if (rc) return rc;
+  e->h_row = std::move(c.row);
+  e->h_so = std::move(c.so);
+  DALLOC(e->d.stdp_log, STDP_LOG_CAP);
+  DALLOC(e->d.stdp_log_cnt, 1);
+  return 0;
+}
+
+extern "C" int dpsnn_stdp_events(dpsnn_engine *e, uint32_t *t_ms, uint32_t *pre, uint32_t *post, float *contribution,
+                                 uint32_t cap, uint32_t *count) {
+  if (!e) return dpsnn_fail(DPSNN_E_PARAM, "null engine");
+  if (!e->d.stdp_log) return dpsnn_fail(DPSNN_E_PARAM, "the STDP event log is not enabled");
+  if (e->stdp_log_t == UINT32_MAX) return dpsnn_fail(DPSNN_E_PARAM, "no step has run yet");
+  int rc = dpsnn_sync(e);   // also reports a full log (DPSNN_E_CAPACITY)
+  if (rc) return rc;
+  uint32_t n = 0;
+  CK(cudaMemcpy(&n, e->d.stdp_log_cnt, 4, cudaMemcpyDeviceToHost));
+  if (n > STDP_LOG_CAP) return dpsnn_fail(DPSNN_E_CAPACITY, "more than %u STDP events in one step", STDP_LOG_CAP);
+  std::vector<uint4> rec(n);
+  if (n) CK(cudaMemcpy(rec.data(), e->d.stdp_log, 16ull * n, cudaMemcpyDeviceToHost));
+  // presynaptic neuron and delay of each record's synapse from the CSR, then
+  // the reference's order: causal events (detection, ascending post, each
+  // post's synapses in backward-list order: delay, then presynaptic neuron,
+  // then generation order), then anti-causal events (delivery: delay
+  // descending, then presynaptic neuron, then generation order)
+  const uint32_t D = e->hnet.D;
+  struct Ev {
+    uint64_t key0, key1;
+    uint32_t pre, post;
+    float c;
+  };
+  std::vector<Ev> ev(n);
+  for (uint32_t i = 0; i < n; i++) {
+    const uint64_t k = (uint64_t)rec[i].x | ((uint64_t)rec[i].y << 32);
+    const uint32_t P = (uint32_t)(std::upper_bound(e->h_row.begin(), e->h_row.end(), k) - e->h_row.begin()) - 1;
+    uint32_t dl = 0;
+    while (dl + 1 < D && e->h_row[P] + e->h_so[(size_t)P * (D + 1) + dl + 1] <= k) dl++;
+    const uint32_t j = rec[i].z & 0x7fffffffu, anti = rec[i].z >> 31;
+    Ev &v = ev[i];
+    v.pre = P;
+    v.post = j;
+    memcpy(&v.c, &rec[i].w, 4);
+    if (anti) {
+      v.key0 = (1ull << 63) | (uint64_t)(D - 1 - dl);
+    } else {
+      v.key0 = ((uint64_t)j << 8) | dl;
+    }
+    v.key1 = k;
+  }
+  std::sort(ev.begin(), ev.end(), [](const Ev &a, const Ev &b) {
+    return a.key0 != b.key0 ? a.key0 < b.key0 : a.key1 < b.key1;
+  });
+  if (t_ms) *t_ms = e->stdp_log_t;
+  if (count) *count = n;
+  const uint32_t m = std::min(n, cap);
+  for (uint32_t i = 0; i < m; i++) {
+    if (pre) pre[i] = ev[i].pre;
+    if (post) post[i] = ev[i].post;
+    if (contribution) contribution[i] = ev[i].c;
+  }
   return 0;
 }
 

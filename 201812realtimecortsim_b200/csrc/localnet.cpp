@@ -1,6 +1,9 @@
 // localnet.cpp -- the DAL process trio of DPSNN over the B200 engine, and
 // the reference's per-rank output files (spikes, ratesPerPop,
-// FiringsInChronoWindow) written from the engine's spike lists.
+// FiringsInChronoWindow) written from the engine's spike lists, and the
+// synapse periodic probe files (synPeriodicProbe_A/B, DPSNN_stat.c:429-449)
+// written from the engine's LTP probe, and the STDP event files (STDPevent,
+// DPSNN_stat.c:451-477) written from the engine's STDP event log.
 //
 // Output formats restate DPSNN_stat.c (file names :66-83, spikes :290-308,
 // ratesPerPop :227-275, open/close windows :594-745) and
@@ -43,6 +46,20 @@ struct LocalNet {
   std::vector<RankStat> rank;
   std::vector<uint32_t> ids;
   std::vector<double> te;
+  // synapse periodic probe (rank 0 only): files, window, and rank 0's
+  // synapses with a presynaptic neuron of rank 0, as indices into its list
+  bool probe = false;
+  uint32_t probe_start_s = 0, probe_stop_s = 0;
+  FILE *probe_a = nullptr, *probe_b = nullptr;
+  std::vector<uint64_t> probe_idx;
+  std::vector<uint32_t> syn_pre, syn_post;
+  std::vector<uint8_t> syn_delay, syn_kind;
+  // STDP event file (rank 0 only)
+  bool stdp_ev = false;
+  uint32_t stdp_start_s = 0, stdp_stop_s = 0, debug_ms = 0;
+  FILE *stdp_f = nullptr;
+  std::vector<uint32_t> ev_pre, ev_post;
+  std::vector<float> ev_c;
 };
 
 LocalNet *g_net = nullptr;
@@ -90,12 +107,70 @@ void open_second(LocalNet &n, uint32_t sec) {
     if (!n.par.statRatesPerPop_writeDisable && rates_second(n.par, sec))
       r.rates = open_stat(n, "ratesPerPop", sec, h);
   }
+  if (n.probe && stat_second(n.par, sec) && sec >= n.probe_start_s && sec <= n.probe_stop_s) {
+    n.probe_a = open_stat(n, "synPeriodicProbe_A", sec, 0);
+    n.probe_b = open_stat(n, "synPeriodicProbe_B", sec, 0);
+  }
+  if (n.stdp_ev && stat_second(n.par, sec) && sec >= n.stdp_start_s && sec <= n.stdp_stop_s)
+    n.stdp_f = open_stat(n, "STDPevent", sec, 0);
 }
 
 void close_second(LocalNet &n) {
   for (RankStat &r : n.rank) {
     close_stat(r.spikes);
     close_stat(r.rates);
+  }
+  close_stat(n.probe_a);
+  close_stat(n.probe_b);
+  close_stat(n.stdp_f);
+}
+
+// The STDP event lines of the step just run (statSTDPeventClass::write,
+// DPSNN_stat.c:451-477), in the order the reference makes them.
+void write_stdp_events(LocalNet &n) {
+  uint32_t t = 0, cnt = 0;
+  if (dpsnn_stdp_events(n.eng, &t, n.ev_pre.data(), n.ev_post.data(), n.ev_c.data(), (uint32_t)n.ev_pre.size(),
+                        &cnt))
+    die("statSTDPevent");
+  if (t != (uint32_t)n.ms) {
+    printf("ERROR STDP events of step %u read at step %d\n", t, n.ms);
+    fflush(stdout);
+    exit(0);
+  }
+  const uint32_t ms = (uint32_t)n.ms;
+  if (n.debug_ms != 0 && !(ms >= n.debug_ms && ms <= n.debug_ms + 20)) return;
+  for (uint32_t i = 0; i < cnt; i++)
+    fprintf(n.stdp_f, "%8u %7d %7d %2.7f \n", ms, (int)n.ev_pre[i], (int)n.ev_post[i], n.ev_c[i]);
+  fflush(n.stdp_f);
+}
+
+// The two probe files of an x999 ms step that ran the plasticity update:
+// rank 0's synapses from rank-0 neurons in backward-list order, in the
+// instrumentedSynapse::report format (DPSNN_synapse.h:63-80), before the
+// update (A) and after it, before the decay of the time derivative (B).
+void write_probe(LocalNet &n) {
+  const uint64_t S = n.syn_pre.size();
+  std::vector<int16_t> wb(S), wa(S);
+  std::vector<float> tb(S), ta(S);
+  uint32_t t = 0;
+  if (dpsnn_ltp_probe(n.eng, 0, &t, wb.data(), tb.data(), wa.data(), ta.data())) die("longTermPlasticity");
+  if (t != (uint32_t)n.ms) {
+    printf("ERROR synapse probe of step %u read at step %d\n", t, n.ms);
+    fflush(stdout);
+    exit(0);
+  }
+  const float w2f = n.par.min_syn_weight_f / -32767;
+  for (int side = 0; side < 2; side++) {
+    FILE *f = side ? n.probe_b : n.probe_a;
+    const int16_t *w = side ? wa.data() : wb.data();
+    const float *td = side ? ta.data() : tb.data();
+    for (uint64_t k : n.probe_idx) {
+      fprintf(f, "%d %d %d %d %d %f ", (int)n.syn_pre[k], (int)n.syn_post[k], (int)(n.syn_post[k] / n.locN),
+              (int)n.syn_delay[k], (int)n.syn_kind[k], (float)(w[k] * w2f));
+      fprintf(f, "%f", td[k]);
+      fprintf(f, "\n");
+    }
+    fflush(f);
   }
 }
 
@@ -249,12 +324,6 @@ void localNetProcess_init(DALProcess *p) {
   }
   LocalNet *n = new LocalNet();
   if (dpsnn_params_from_env(nullptr, &n->par)) die("getParameters");
-  // side outputs of the reference that this process does not write
-  for (const char *v : {"env_statSTDPevent_writeDisable", "env_statSynPeriodicProbe_writeDisable"}) {
-    const char *s = getenv(v);
-    if (s && atoi(s) == 0)
-      fprintf(stderr, "WARNING %s=0: those statistics files are not written by this engine\n", v);
-  }
   const dpsnn_params &q = n->par;
   n->P = q.glob_h;
   n->globCFT = q.cfx * q.cfy;
@@ -267,6 +336,35 @@ void localNetProcess_init(DALProcess *p) {
   memset(&opt, 0, sizeof opt);
   opt.device = (int)env_u32_or("DPSNN_DEVICE", 0);
   if (dpsnn_create(&n->par, &opt, &n->eng)) die("localNetClass::init");
+  // statClass::prep (DPSNN_stat.c:553-561): only rank 0 writes the probe
+  n->probe = env_u32_or("env_statSynPeriodicProbe_writeDisable", 1) == 0;
+  n->probe_start_s = env_u32_or("env_startSynPeriodicProbe_s", 0);
+  n->probe_stop_s = env_u32_or("env_stopSynPeriodicProbe_s", 0);
+  if (n->probe && q.start_plasticity_ms <= q.stop_plasticity_ms && q.start_plasticity_ms < q.total_sim_time_ms) {
+    if (dpsnn_enable_ltp_probe(n->eng)) die("statSynPeriodicProbe");
+    const uint64_t S = dpsnn_rank_synapse_count(n->eng, 0);
+    n->syn_pre.resize(S);
+    n->syn_post.resize(S);
+    n->syn_delay.resize(S);
+    n->syn_kind.resize(S);
+    if (dpsnn_backward_synapses(n->eng, 0, n->syn_pre.data(), n->syn_post.data(), n->syn_delay.data(),
+                                n->syn_kind.data(), nullptr, nullptr))
+      die("statSynPeriodicProbe");
+    for (uint64_t k = 0; k < S; k++)
+      if (n->syn_pre[k] < n->locN) n->probe_idx.push_back(k);
+  }
+  // statClass::prep (DPSNN_stat.c:546-551): only rank 0 writes STDP events
+  n->stdp_ev = env_u32_or("env_statSTDPevent_writeDisable", 1) == 0 && q.start_plasticity_ms <= q.stop_plasticity_ms &&
+               q.start_plasticity_ms < q.total_sim_time_ms;
+  n->stdp_start_s = env_u32_or("env_startSTDPevent_s", 0);
+  n->stdp_stop_s = env_u32_or("env_stopSTDPevent_s", 0);
+  n->debug_ms = env_u32_or("env_debugPrintEnable_ms", 0);
+  if (n->stdp_ev) {
+    if (dpsnn_enable_stdp_events(n->eng)) die("statSTDPevent");
+    n->ev_pre.resize(DPSNN_STDP_LOG_CAP);
+    n->ev_post.resize(DPSNN_STDP_LOG_CAP);
+    n->ev_c.resize(DPSNN_STDP_LOG_CAP);
+  }
   n->max_ms = (int32_t)q.total_sim_time_ms;
   n->chrono = env_u32_or("env_chrono", 0);
   n->chrono_start = env_u32_or("env_startPartialChrono_ms", 0);
@@ -306,6 +404,13 @@ int localNetProcess_fire(DALProcess *p) {
     rank_outputs(*n, h, n->ids.data() + a, n->te.data() + a, b - a);
     a = b;
   }
+  if (n->stdp_f) write_stdp_events(*n);
+  // longTermPlasticity runs at x999 ms inside the plasticity window
+  // (DPSNN_localNet_sim.c:281-284) and writes the probe
+  const dpsnn_params &q = n->par;
+  if (n->ms % 1000 == 999 && n->probe_a && !n->syn_pre.empty() && (uint32_t)n->ms >= q.start_plasticity_ms &&
+      (uint32_t)n->ms <= q.stop_plasticity_ms)
+    write_probe(*n);
   if (n->ms % 1000 == 999) close_second(*n);
   n->ms++;
   return 0;

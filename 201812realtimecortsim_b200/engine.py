@@ -55,10 +55,12 @@ EXPORTS = [
     "dpsnn_glob_n", "dpsnn_time_ms", "dpsnn_synapse_count", "dpsnn_events_delivered",
     "dpsnn_spikes", "dpsnn_rank_synapse_count", "dpsnn_backward_synapses", "dpsnn_state",
     "dpsnn_bath_params", "dpsnn_set_timing", "dpsnn_kernel_times", "dpsnn_kernel_launches", "dpsnn_cuda_stream",
-    "dpsnn_rank_spikes_noalloc", "dpsnn_last_error",
+    "dpsnn_rank_spikes_noalloc", "dpsnn_enable_ltp_probe", "dpsnn_ltp_probe",
+    "dpsnn_enable_stdp_events", "dpsnn_stdp_events", "dpsnn_last_error",
 ]
 NOALLOC_MAX_SPIKES = 32768   # DPSNN_NOALLOC_MAX_SPIKES
 TIMING_SLOTS = 8             # DPSNN_TIMING_SLOTS
+STDP_LOG_CAP = 1 << 21       # DPSNN_STDP_LOG_CAP
 TIMING_NAMES = ["compact", "deliver", "bath", "neuron", "plasticity", "heavy_sort", "heavy_run", "huge"]
 
 _LIB = None
@@ -101,6 +103,10 @@ def load_library(path: str = LIB_PATH):
     lib.dpsnn_cuda_stream.restype = C.c_void_p
     lib.dpsnn_rank_spikes_noalloc.argtypes = [P, C.c_uint32, C.c_uint32, P, P, C.c_uint32,
                                               C.POINTER(C.c_uint32)]
+    lib.dpsnn_enable_ltp_probe.argtypes = [P]
+    lib.dpsnn_ltp_probe.argtypes = [P, C.c_uint32, C.POINTER(C.c_uint32)] + [P] * 4
+    lib.dpsnn_enable_stdp_events.argtypes = [P]
+    lib.dpsnn_stdp_events.argtypes = [P, C.POINTER(C.c_uint32), P, P, P, C.c_uint32, C.POINTER(C.c_uint32)]
     lib.dpsnn_last_error.restype = C.c_char_p
     _LIB = lib
     return lib
@@ -246,6 +252,36 @@ class Engine:
         self._check(self._L.dpsnn_backward_synapses(self._h, rank, _ptr(pre), _ptr(post), _ptr(d), _ptr(k),
                                                      _ptr(w), _ptr(td)), "dpsnn_backward_synapses")
         return (pre, post, d, k, w, td) if with_tderiv else (pre, post, d, k, w)
+
+    def enable_ltp_probe(self):
+        """Keep the synapses around each plasticity update (before the first step)."""
+        self._check(self._L.dpsnn_enable_ltp_probe(self._h), "dpsnn_enable_ltp_probe")
+
+    def ltp_probe(self, rank: int = 0):
+        """(step, w_before, td_before, w_after, td_after) of the last plasticity
+        update, in the order of :meth:`backward_synapses`."""
+        n = self._L.dpsnn_rank_synapse_count(self._h, rank)
+        wb, wa = np.empty(n, np.int16), np.empty(n, np.int16)
+        tb, ta = np.empty(n, np.float32), np.empty(n, np.float32)
+        t = C.c_uint32(0)
+        self._check(self._L.dpsnn_ltp_probe(self._h, rank, C.byref(t), _ptr(wb), _ptr(tb), _ptr(wa), _ptr(ta)),
+                    "dpsnn_ltp_probe")
+        return t.value, wb, tb, wa, ta
+
+    def enable_stdp_events(self):
+        """Log every step's rank-0 STDP contributions (before the first step)."""
+        self._check(self._L.dpsnn_enable_stdp_events(self._h), "dpsnn_enable_stdp_events")
+
+    def stdp_events(self):
+        """(step, pre, post, contribution) of the last step queued, in the
+        reference's order."""
+        cap = STDP_LOG_CAP
+        pre, post = np.empty(cap, np.uint32), np.empty(cap, np.uint32)
+        c = np.empty(cap, np.float32)
+        t, n = C.c_uint32(0), C.c_uint32(0)
+        self._check(self._L.dpsnn_stdp_events(self._h, C.byref(t), _ptr(pre), _ptr(post), _ptr(c), cap,
+                                              C.byref(n)), "dpsnn_stdp_events")
+        return t.value, pre[:n.value].copy(), post[:n.value].copy(), c[:n.value].copy()
 
     def state(self):
         arrs = [np.empty(self.glob_n, np.float64) for _ in range(5)]

@@ -20,7 +20,10 @@
  *   dpsnn_spikes           <- the spike list handed to statSpikesClass::write
  *                                                         DPSNN_localNet_sim.c:222-226
  *   dpsnn_backward_synapses<- backwardSynList of rank h   DPSNN_localNet_init.c:591-617
- *   dpsnn_destroy          <- process exit (the reference never frees)
+ *   dpsnn_ltp_probe        <- the synPeriodicProbe_A/B records
+ *                                                         DPSNN_localNet_sim.c:360-397
+ *   dpsnn_stdp_events      <- the STDPevent records       DPSNN_neuron_sim.c:152-166,230-246
+ *   dpsnn_destroy         <- process exit (the reference never frees)
  * The DAL process trio localNetProcess_init/fire/finish and getParameters
  * themselves, with C++ linkage as in the reference, are exported by
  * libdpsnn_localnet.so (dpsnn_localnet.h).
@@ -134,6 +137,37 @@ int dpsnn_spikes(dpsnn_engine *e, uint32_t t_ms, uint32_t *ids, double *te,
 uint64_t dpsnn_rank_synapse_count(dpsnn_engine *e, uint32_t h);
 int dpsnn_backward_synapses(dpsnn_engine *e, uint32_t h, uint32_t *pre, uint32_t *post,
                             uint8_t *delay, uint8_t *kind, int16_t *weight, float *tderiv);
+
+/* LTP probe: the synapses just before and just after each once-per-second
+ * plasticity update, the records statSynPeriodicProbeA/B write inside
+ * longTermPlasticity (DPSNN_localNet_sim.c:360-364 and :391-397).
+ * dpsnn_enable_ltp_probe allocates 10 B per synapse on the device; it is
+ * called before the first step, on an engine with plasticity switched on.
+ * dpsnn_ltp_probe waits for the queued steps, then returns, for the last
+ * update run (its step in *t_ms), rank h's synapses in the order of
+ * dpsnn_backward_synapses: the weight and time derivative before the update,
+ * and the weight and time derivative after it, the latter before its
+ * decay.  Any array pointer may be NULL. */
+int dpsnn_enable_ltp_probe(dpsnn_engine *e);
+int dpsnn_ltp_probe(dpsnn_engine *e, uint32_t h, uint32_t *t_ms, int16_t *w_before, float *td_before,
+                    int16_t *w_after, float *td_after);
+
+/* STDP event log: the records statSTDPevent writes on rank 0
+ * (DPSNN_neuron_sim.c:152-166, causal, and :230-246, anti-causal): every
+ * non-zero STDP contribution on a synapse of rank 0 whose presynaptic and
+ * postsynaptic neurons are both rank-0 neurons.  dpsnn_enable_stdp_events
+ * allocates the log (32 MiB, 2^21 records a step) before the first step, on an
+ * engine with plasticity switched on.  The log holds the last step queued:
+ * dpsnn_stdp_events waits for it and returns its step in *t_ms and its
+ * records in the reference's order (causal events by ascending postsynaptic
+ * neuron, each neuron's synapses in backward-list order; then anti-causal
+ * events in delivery order); *count receives the number of records, at most
+ * cap are written.  A step with more records fails with DPSNN_E_CAPACITY.
+ * Read it after every dpsnn_step(e, 1) to see every step. */
+#define DPSNN_STDP_LOG_CAP (1u << 21)
+int dpsnn_enable_stdp_events(dpsnn_engine *e);
+int dpsnn_stdp_events(dpsnn_engine *e, uint32_t *t_ms, uint32_t *pre, uint32_t *post, float *contribution,
+                      uint32_t cap, uint32_t *count);
 
 /* Neuron state, global neuron index order; any pointer may be NULL. */
 int dpsnn_state(dpsnn_engine *e, double *v, double *c, double *tr, double *te, double *nb);

@@ -14,10 +14,14 @@ built from the unmodified sources plus the bounds fix:
 * ``<case>.spikes.gz``   the reference's own spikes file (%.7g);
 * ``manifest.json``      sha256 of the BACKWARD synapse dump and of the
                           output files (spikes, ratesPerPop,
-                          FiringsInChronoWindow), spike and synaptic-event
-                          counts, configuration.
+                          FiringsInChronoWindow; with plasticity also the
+                          synapse periodic probe files synPeriodicProbe_A/B
+                          and the STDPevent files, from a run that enables
+                          them),
+                          spike and synaptic-event counts, configuration.
 
-Usage: python tests/golden/make_golden.py
+Usage: python tests/golden/make_golden.py [case ...]
+(with case names, only those entries of the manifest are regenerated)
 """
 import gzip
 import hashlib
@@ -47,6 +51,10 @@ REF_EXP = os.path.join(ROOT, "oracle", "_ref", "dpsnn_ref_exp")
 # the Perseo .ini writer switched on (compiled out of the stock build)
 REF_INI = os.path.join(ROOT, "oracle", "_ref", "dpsnn_ref_ini")
 KAT = os.path.join(ROOT, "oracle", "_ref", "ref_kat")
+# the side outputs of a plasticity run: synapse probe and STDP event files
+PROBE_ENV = {"env_statSynPeriodicProbe_writeDisable": "0", "env_startSynPeriodicProbe_s": "0",
+             "env_stopSynPeriodicProbe_s": "100000", "env_statSTDPevent_writeDisable": "0",
+             "env_startSTDPevent_s": "0", "env_stopSTDPevent_s": "100000"}
 
 
 def sha256(path):
@@ -80,8 +88,14 @@ def main():
                    capture_output=True)
     with open(os.path.join(HERE, "ref_kat.txt"), "w") as f:
         f.write(subprocess.run([KAT], check=True, capture_output=True, text=True).stdout)
+    only = sys.argv[1:]
     manifest = {}
+    if only:
+        with open(os.path.join(HERE, "manifest.json")) as f:
+            manifest = json.load(f)
     for name, make in CASES.items():
+        if only and name not in only:
+            continue
         cfg = make()
         entry = {"total_ms": cfg.total_ms, "glob_h": cfg.glob_h}
         with tempfile.TemporaryDirectory() as td:
@@ -111,6 +125,15 @@ def main():
                 for h in range(cfg.glob_h):
                     with open(os.path.join(std, f"spikes-sec0-C{cfg.n_modules}-H{cfg.glob_h}-h{h:03d}.dat")) as g:
                         f.write(g.read())
+            if cfg.stdp is not None:
+                pr = os.path.join(td, "probe")
+                probe = make()
+                probe.extra_env.update(PROBE_ENV)
+                run(REF, probe, pr)
+                entry["probe_sha256"] = {fn: sha256(os.path.join(pr, fn)) for fn in sorted(os.listdir(pr))
+                                         if fn.startswith("synPeriodicProbe_")}
+                entry["stdp_event_sha256"] = {fn: sha256(os.path.join(pr, fn)) for fn in sorted(os.listdir(pr))
+                                              if fn.startswith("STDPevent-")}
             if cfg.glob_h == 1 and not cfg.delay_exponential:
                 ini = os.path.join(td, "ini")
                 short = make()

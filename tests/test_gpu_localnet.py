@@ -74,3 +74,26 @@ def test_trio_writes_every_emulated_rank(tmp_path):
         want += [(int(i), "%.7g" % t) for i, t in zip(ids, ts)]
     assert len(want) > 0
     assert sorted(got) == sorted(want)
+
+
+@pytest.mark.parametrize("name", [n for n, e in sorted(gio.manifest().items()) if "probe_sha256" in e])
+def test_trio_plasticity_side_files_identical_to_reference(name, tmp_path):
+    """With the synapse probe and STDP event switches on, the trio writes rank
+    0's synPeriodicProbe_A/B files (synapses before and after each x999 ms
+    plasticity update) and its STDPevent files (every causal and anti-causal
+    contribution between rank-0 neurons, in the reference's order), byte for
+    byte as the reference does; the other output files stay identical too."""
+    cfg = CASES[name]()
+    cfg.extra_env.update({"env_statSynPeriodicProbe_writeDisable": "0",
+                          "env_startSynPeriodicProbe_s": "0",
+                          "env_stopSynPeriodicProbe_s": "100000",
+                          "env_statSTDPevent_writeDisable": "0",
+                          "env_startSTDPevent_s": "0",
+                          "env_stopSTDPevent_s": "100000"})
+    run_in(RUNNER, cfg, str(tmp_path))
+    entry = gio.manifest()[name]
+    want = dict(entry["probe_sha256"], **entry["stdp_event_sha256"], **entry["outputs_sha256"])
+    side = sorted(fn for fn in os.listdir(tmp_path) if fn.startswith(("synPeriodicProbe_", "STDPevent-")))
+    assert side == sorted(list(entry["probe_sha256"]) + list(entry["stdp_event_sha256"]))
+    got = {fn: sha256(os.path.join(tmp_path, fn)) for fn in want if os.path.exists(os.path.join(tmp_path, fn))}
+    assert got == want
