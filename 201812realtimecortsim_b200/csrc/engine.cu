@@ -2376,6 +2376,22 @@ extern "C" int dpsnn_step(dpsnn_engine *e, uint32_t nsteps) {
   return 0;
 }
 
+extern "C" int dpsnn_step_many(dpsnn_engine *const *engines, uint32_t n, uint32_t nsteps) {
+  if (!engines && n) return dpsnn_fail(DPSNN_E_PARAM, "null engine array");
+  for (uint32_t i = 0; i < n; i++)
+    if (!engines[i]) return dpsnn_fail(DPSNN_E_PARAM, "null engine %u", i);
+  // one step of every engine in turn: each engine's kernels queue on its own
+  // streams, so the networks' steps overlap on the device
+  for (uint32_t k = 0; k < nsteps; k++)
+    for (uint32_t i = 0; i < n; i++) {
+      dpsnn_engine *e = engines[i];
+      cudaSetDevice(e->device);
+      int rc = enqueue_step(e);
+      if (rc) return rc;
+    }
+  return 0;
+}
+
 extern "C" int dpsnn_sync(dpsnn_engine *e) {
   if (!e) return dpsnn_fail(DPSNN_E_PARAM, "null engine");
   cudaSetDevice(e->device);

@@ -56,7 +56,7 @@ EXPORTS = [
     "dpsnn_spikes", "dpsnn_rank_synapse_count", "dpsnn_backward_synapses", "dpsnn_state",
     "dpsnn_bath_params", "dpsnn_set_timing", "dpsnn_kernel_times", "dpsnn_kernel_launches", "dpsnn_cuda_stream",
     "dpsnn_rank_spikes_noalloc", "dpsnn_enable_ltp_probe", "dpsnn_ltp_probe",
-    "dpsnn_enable_stdp_events", "dpsnn_stdp_events", "dpsnn_last_error",
+    "dpsnn_enable_stdp_events", "dpsnn_stdp_events", "dpsnn_step_many", "dpsnn_last_error",
 ]
 NOALLOC_MAX_SPIKES = 32768   # DPSNN_NOALLOC_MAX_SPIKES
 TIMING_SLOTS = 8             # DPSNN_TIMING_SLOTS
@@ -107,6 +107,7 @@ def load_library(path: str = LIB_PATH):
     lib.dpsnn_ltp_probe.argtypes = [P, C.c_uint32, C.POINTER(C.c_uint32)] + [P] * 4
     lib.dpsnn_enable_stdp_events.argtypes = [P]
     lib.dpsnn_stdp_events.argtypes = [P, C.POINTER(C.c_uint32), P, P, P, C.c_uint32, C.POINTER(C.c_uint32)]
+    lib.dpsnn_step_many.argtypes = [P, C.c_uint32, C.c_uint32]
     lib.dpsnn_last_error.restype = C.c_char_p
     _LIB = lib
     return lib
@@ -323,3 +324,13 @@ def params_from_env(workdir: str) -> ParamsHolder:
     p.spec = spec.ctypes.data_as(C.POINTER(C.c_float))
     p.bath = bath.ctypes.data_as(C.POINTER(C.c_uint32))
     return ParamsHolder(p, spec, bath)
+
+
+def step_many(engines, n: int):
+    """The batched form: ``n`` steps of each engine, queued one step of every
+    engine at a time so that independent networks overlap on the device."""
+    lib = load_library()
+    arr = (C.c_void_p * len(engines))(*[e._h for e in engines])
+    rc = lib.dpsnn_step_many(arr, len(engines), n)
+    if rc != 0:
+        raise EngineError(f"dpsnn_step_many failed ({rc}): {lib.dpsnn_last_error().decode()}")

@@ -204,6 +204,63 @@ def run_reference(args, world, rank):
     }))
 
 
+def batch_jobs(n_jobs: int, ms: int):
+    """The batched sweep: independent networks of 1x1 to 4x4 modules (uniform),
+    each with its own seed, external Poisson rate (1-5 kHz: NuExt 1-5 Hz over
+    CExt 1000) and calcium adaptation increment (0-2x the baseline 1.0)."""
+    import numpy as np
+    nc = importlib.import_module("201812realtimecortsim_b200.netconfig")
+    rng = np.random.default_rng(2024)
+    jobs = []
+    for i in range(n_jobs):
+        g = int(rng.integers(1, 5))
+        nu, alpha = float(rng.uniform(1.0, 5.0)), float(rng.uniform(0.0, 2.0))
+        kw = {"p1": 0.0376} if g <= 2 else {}
+        jobs.append(nc.cortical_grid(g, g, total_ms=ms + 10, seed=1 + i, nu_ext_hz=nu, alpha_c=alpha, **kw))
+    return jobs
+
+
+def run_batch(args):
+    """One JSON line for the batched form: the jobs run together through
+    dpsnn_step_many against the same jobs issued one at a time with
+    dpsnn_step, each arm on freshly built engines, host wall time between
+    device synchronisations (the arms span many streams)."""
+    import torch
+    E = importlib.import_module("201812realtimecortsim_b200.engine")
+    jobs = batch_jobs(args.batch, args.batch_ms)
+    res = {}
+    for arm in ("sequential", "batched"):
+        engines = [E.Engine(c, device=0) for c in jobs]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if arm == "sequential":
+            for e in engines:
+                e.step(args.batch_ms)
+                e.sync()
+        else:
+            E.step_many(engines, args.batch_ms)
+            for e in engines:
+                e.sync()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        ev = [e.events_delivered() for e in engines]
+        res[arm] = (dt, ev)
+        for e in engines:
+            e.close()
+        del engines
+    (ts, evs), (tb, evb) = res["sequential"], res["batched"]
+    neurons = sum(c.glob_n for c in jobs)
+    print(json.dumps({
+        "metric": "aggregate synaptic events/s (batched sweep)", "value": sum(evb) / tb, "unit": UNIT,
+        "n_gpus": 1, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{len(jobs)} independent networks of 1x1-4x4 modules ({neurons} neurons), "
+                               f"{args.batch_ms} ms each, per-job seed, NuExt 1-5 Hz, AlphaC 0-2, STDP off",
+                   "timing": "host wall time between device synchronisations"},
+        "batched_s": tb, "sequential_s": ts, "sequential_value": sum(evs) / ts,
+        "per_job_events_identical": evs == evb,
+    }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -214,7 +271,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", default="24x24", help="CFXxCFY modules (profiling of smaller grids)")
     ap.add_argument("--ranks", type=int, default=192, help="env_globH: emulated reference ranks")
+    ap.add_argument("--batch", type=int, default=0, help="run the batched sweep of this many networks instead")
+    ap.add_argument("--batch-ms", type=int, default=2000, help="biological ms per network in the batched sweep")
     args = ap.parse_args()
+    if args.batch:
+        run_batch(args)
+        return
     args.warmup = max(args.warmup, 3)
     world, rank, local, dist = dist_setup(args)
     if args.impl == "reference":

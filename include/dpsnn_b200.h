@@ -113,6 +113,11 @@ void dpsnn_destroy(dpsnn_engine *e);
 /* Run nsteps 1 ms steps (asynchronously; results are read by the calls below,
  * which synchronise). */
 int dpsnn_step(dpsnn_engine *e, uint32_t nsteps);
+/* Batched form: nsteps steps of each of n independent engines, queued one
+ * step of every engine at a time, so that their kernels overlap on the
+ * device; each engine's results are those of dpsnn_step on it alone.
+ * Asynchronous like dpsnn_step. */
+int dpsnn_step_many(dpsnn_engine *const *engines, uint32_t n, uint32_t nsteps);
 /* Block until all queued steps are done; reports a deferred device error. */
 int dpsnn_sync(dpsnn_engine *e);
 
