@@ -14,6 +14,10 @@ value  = synaptic events delivered in the K steps / device time (CUDA events
 e2e    = the same metric through the C ABI as a drop-in caller uses it: one
          dpsnn_step per ms and the step's spike list read back to host memory
          (the raster), timed on the host; no per-step input goes to the device.
+--batch J runs the batched sweep instead: J independent networks of 1x1-4x4
+modules, --batch-ms biological ms of each, stepped together (dpsnn_step_many)
+and, on freshly built engines, one after another (dpsnn_step), printing one
+JSON line with both aggregate rates.
 The reference arm (--impl reference) runs the reference binary built from the
 reference sources (oracle/_ref/dpsnn_ref) on the host cores: one single-rank
 process per core, each simulating the 2x2 network (the reference's
@@ -229,14 +233,25 @@ def run_batch(args):
     E = importlib.import_module("201812realtimecortsim_b200.engine")
     jobs = batch_jobs(args.batch, args.batch_ms)
     res = {}
+    build_s = {}
     for arm in ("sequential", "batched"):
-        engines = [E.Engine(c, device=0) for c in jobs]
-        torch.cuda.synchronize()
+        tb0 = time.perf_counter()
+        engines = []
+        for c in jobs:   # progress on stderr: which phase and job size take the time
+            tj = time.perf_counter()
+            engines.append(E.Engine(c, device=0))
+            torch.cuda.synchronize()
+            print(f"[batch] {arm}: built {c.cfx}x{c.cfy} ({c.glob_n} neurons) in "
+                  f"{time.perf_counter() - tj:.3f} s", file=sys.stderr, flush=True)
         t0 = time.perf_counter()
+        build_s[arm] = t0 - tb0
         if arm == "sequential":
-            for e in engines:
+            for c, e in zip(jobs, engines):
+                tj = time.perf_counter()
                 e.step(args.batch_ms)
                 e.sync()
+                print(f"[batch] sequential: {c.cfx}x{c.cfy} stepped {args.batch_ms} ms in "
+                      f"{time.perf_counter() - tj:.3f} s", file=sys.stderr, flush=True)
         else:
             E.step_many(engines, args.batch_ms)
             for e in engines:
@@ -256,7 +271,7 @@ def run_batch(args):
         "config": {"workload": f"{len(jobs)} independent networks of 1x1-4x4 modules ({neurons} neurons), "
                                f"{args.batch_ms} ms each, per-job seed, NuExt 1-5 Hz, AlphaC 0-2, STDP off",
                    "timing": "host wall time between device synchronisations"},
-        "batched_s": tb, "sequential_s": ts, "sequential_value": sum(evs) / ts,
+        "batched_s": tb, "sequential_s": ts, "sequential_value": sum(evs) / ts, "build_s": build_s,
         "per_job_events_identical": evs == evb,
     }), flush=True)
 
@@ -272,7 +287,8 @@ def main():
     ap.add_argument("--grid", default="24x24", help="CFXxCFY modules (profiling of smaller grids)")
     ap.add_argument("--ranks", type=int, default=192, help="env_globH: emulated reference ranks")
     ap.add_argument("--batch", type=int, default=0, help="run the batched sweep of this many networks instead")
-    ap.add_argument("--batch-ms", type=int, default=2000, help="biological ms per network in the batched sweep")
+    ap.add_argument("--batch-ms", type=int, default=100,
+                    help="biological ms per network timed in the batched sweep (a bounded sample)")
     args = ap.parse_args()
     if args.batch:
         run_batch(args)
