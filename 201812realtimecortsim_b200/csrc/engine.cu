@@ -54,17 +54,16 @@ int dpsnn_fail(int code, const char *fmt, ...) {
 extern "C" const char *dpsnn_last_error(void) { return g_err; }
 
 const char *dpsnn_library_dir(void) {
-  static std::string dir;
-  if (dir.empty()) {
+  // initialised once, thread-safely (engines may be created from several threads)
+  static const std::string dir = [] {
     Dl_info info;
     if (dladdr((void *)&dpsnn_library_dir, &info) && info.dli_fname) {
-      dir = info.dli_fname;
-      size_t p = dir.rfind('/');
-      dir = (p == std::string::npos) ? std::string(".") : dir.substr(0, p);
-    } else {
-      dir = ".";
+      std::string d = info.dli_fname;
+      size_t p = d.rfind('/');
+      return (p == std::string::npos) ? std::string(".") : d.substr(0, p);
     }
-  }
+    return std::string(".");
+  }();
   return dir.c_str();
 }
 
@@ -1999,11 +1998,10 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
   CK(cudaStreamSynchronize(e->stream));
   for (uint32_t m = 0; m < nmod; m++)
     if (recB[m].err) return dpsnn_fail(DPSNN_E_MODEL, "synapse generation pass B error %d", recB[m].err);
-  // free generation scratch
-  for (void *q : {(void *)cnt_out, (void *)scratch, (void *)row_len, (void *)bath_tmpl}) {
-    cudaFree(q);
-    e->allocs.erase(std::find(e->allocs.begin(), e->allocs.end(), q));
-  }
+  // The generation scratch (cnt_out, scratch, row_len, bath_tmpl) stays
+  // allocated until dpsnn_destroy: cudaFree waits for the whole device, so
+  // freeing here would serialise builds issued from several host threads
+  // behind each other's generation kernels.
   // ---- run-over-group-end check (see DPSNN_synapse.c:211-265): the reference's
   // search continues past a (delay, source rank) group while the next entry has
   // the same presynaptic index; this happens only when the last source of a
@@ -2146,8 +2144,7 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
   }
   int rc = load_logf_fixup(e);
   if (rc) return rc;
-  cudaFree(dprob);
-  e->allocs.erase(std::find(e->allocs.begin(), e->allocs.end(), (void *)dprob));
+  // dprob too stays allocated until dpsnn_destroy (no device-wide cudaFree)
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
   e->grid_deliver = (uint32_t)sms * 8;

@@ -27,6 +27,7 @@ committed fixture of that run.
 from __future__ import annotations
 
 import argparse
+import concurrent.futures
 import importlib
 import json
 import os
@@ -236,13 +237,20 @@ def run_batch(args):
     build_s = {}
     for arm in ("sequential", "batched"):
         tb0 = time.perf_counter()
-        engines = []
-        for c in jobs:   # progress on stderr: which phase and job size take the time
+
+        def build(c):
+            # a build is seconds of serial per-module ran3 streams on a few GPU
+            # threads whatever the network's size: builds from several host
+            # threads overlap (the engine call releases the GIL)
             tj = time.perf_counter()
-            engines.append(E.Engine(c, device=0))
-            torch.cuda.synchronize()
+            e = E.Engine(c, device=0)
             print(f"[batch] {arm}: built {c.cfx}x{c.cfy} ({c.glob_n} neurons) in "
                   f"{time.perf_counter() - tj:.3f} s", file=sys.stderr, flush=True)
+            return e
+
+        with concurrent.futures.ThreadPoolExecutor(max_workers=min(32, len(jobs))) as pool:
+            engines = list(pool.map(build, jobs))
+        torch.cuda.synchronize()
         t0 = time.perf_counter()
         build_s[arm] = t0 - tb0
         if arm == "sequential":
