@@ -179,10 +179,14 @@ __device__ static inline double normdev(Ran3 &g, NormState &ns) {
   return ns.cache;
 }
 
-__host__ __device__ static inline uint32_t roundr2i(double r) {  // erflib.c:172-181
+// erflib.c:172-181.  The reference converts a possibly negative double to
+// uint32_t; its x86-64 build truncates to 64 bits and keeps the low 32 bits
+// (so -1.0 gives 0xFFFFFFFF), which the two casts state explicitly (a plain
+// device cast would saturate to 0).
+__host__ __device__ static inline uint32_t roundr2i(double r) {
   double i = floor(r);
-  if (i + 0.5 > r) return (uint32_t)i;
-  return (uint32_t)(i + 1.0);
+  if (i + 0.5 > r) return (uint32_t)(int64_t)i;
+  return (uint32_t)(int64_t)(i + 1.0);
 }
 
 __device__ static inline uint32_t subpop_of(const NetConst *net, uint32_t in_cm) {
@@ -210,7 +214,7 @@ struct GenRecord {
 };
 
 enum { GEN_ERR_TOO_MANY = 1, GEN_ERR_WEIGHT_RANGE = 2, GEN_ERR_PROB = 3, GEN_ERR_DELAY = 4,
-       GEN_ERR_ZERO_MEAN = 5 };
+       GEN_ERR_ZERO_MEAN = 5, GEN_ERR_DELAY_LEVEL = 6, GEN_ERR_DELAY_RANGE = 7 };
 
 __device__ static inline uint32_t empty_random_synapses(Ran3 &g, float pf, uint32_t max_n) {
   // getEmptyRandomSynapses (DPSNN_LIFCAconnectome.cpp:1079-1133)
@@ -225,6 +229,10 @@ __device__ static inline uint32_t empty_random_synapses(Ran3 &g, float pf, uint3
   }
   return n;
 }
+
+// Delay generators' error returns (the reference's exit(0) points).
+#define DELAY_LEVEL_ERR 0xFFFFFFFFu   // level >= DSD__delayNum
+#define DELAY_RANGE_ERR 0xFFFFFFFEu   // delay beyond the pair's DMax
 
 __device__ static inline uint32_t random_delay_uni(const NetConst *net, Ran3 &g, uint32_t s, uint32_t t) {
   // getRandomDelay_UNI (DPSNN_LIFCAcorticalModuleGen.cpp:299-338)
@@ -241,12 +249,17 @@ __device__ static inline uint32_t random_delay_uni(const NetConst *net, Ran3 &g,
   DMin = roundr2i((DMin - DelayMin) / DelayStep) * DelayStep + DelayMin;
   outF = (float)((r3_rand(g) * (DMax - DMin) + DMin - DelayMin) / DelayStep);
   (void)DelayMax;
-  return roundr2i(outF * DelayStep);
+  // the reference stops here: "delay level generated %f > %f max allowed
+  // delay levels" (:322-326); the level goes back in the error argument
+  if (outF >= DelayNum) return DELAY_LEVEL_ERR;
+  const uint32_t outfunc = roundr2i(outF * DelayStep);
+  if (outfunc > net->DMax[s * DPSNN_MAX_SUBPOP + t]) return DELAY_RANGE_ERR;   // :330-334
+  return outfunc;
 }
 
 // getRandomDelay_EXP (DPSNN_LIFCAcorticalModuleGen.cpp:247-297), the
 // reference Makefile's default: a truncated exponential over [DMin, DMax);
-// 0xFFFFFFFF where the reference stops with an error.
+// DELAY_LEVEL_ERR / DELAY_RANGE_ERR where the reference stops with an error.
 __device__ static inline uint32_t random_delay_exp(const NetConst *net, Ran3 &g, uint32_t s, uint32_t t) {
   float outfuncF, DMin, DMax, DelayMin, DelayMax, DelayStep, DelayNum;
   const float InvLogTN = net->inv_log_tn;
@@ -263,9 +276,9 @@ __device__ static inline uint32_t random_delay_exp(const NetConst *net, Ran3 &g,
   outfuncF = (float)((((double)DMin + (double)(DMax - DMin - DelayStep) *
                        log_cr(1.0 - r3_rand(g) * (1.0 - 0.05)) * (double)InvLogTN) -
                       (double)DelayMin) / (double)DelayStep);
-  if (outfuncF >= DelayNum) return 0xFFFFFFFFu;
+  if (outfuncF >= DelayNum) return DELAY_LEVEL_ERR;
   const uint32_t outfunc = roundr2i(outfuncF * DelayStep);
-  if (outfunc >= net->DMax[s * DPSNN_MAX_SUBPOP + t]) return 0xFFFFFFFFu;
+  if (outfunc >= net->DMax[s * DPSNN_MAX_SUBPOP + t]) return DELAY_RANGE_ERR;
   (void)DelayMax;
   return outfunc;
 }
@@ -328,6 +341,8 @@ __global__ void gen_kernel(const NetConst *__restrict__ net, const float *__rest
       uint32_t tg = tl[j];
       uint32_t tsub = subpop_of(net, tg % npcm);
       uint32_t delay = net->delay_exp ? random_delay_exp(net, g, ssub, tsub) : random_delay_uni(net, g, ssub, tsub);
+      if (delay == DELAY_LEVEL_ERR) { R->err = GEN_ERR_DELAY_LEVEL; R->err_arg = gi; return; }
+      if (delay == DELAY_RANGE_ERR) { R->err = GEN_ERR_DELAY_RANGE; R->err_arg = gi; return; }
       if (delay >= D) { R->err = GEN_ERR_DELAY; R->err_arg = delay; return; }
       float mean = (float)net->J[ssub * DPSNN_MAX_SUBPOP + tsub];
       float sigma = (float)(net->DJ[ssub * DPSNN_MAX_SUBPOP + tsub] * (double)mean);
@@ -1937,7 +1952,9 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
     if (rec[k].err && !((k & 1) && (k / 2) % n.mods_per_rank == 0)) {
       const char *what[] = {"", "too many synapses generated for neuron", "synaptic weight out of minSynWeight_f range",
                             "connection probability in (0,1e-5] is not supported", "delay >= env_D",
-                            "zero mean synaptic efficacy"};
+                            "zero mean synaptic efficacy",
+                            "ERROR: delay level generated beyond the 80 max allowed delay levels, source neuron",
+                            "ERROR: delay generated beyond the pair's DMax, source neuron"};
       return dpsnn_fail(DPSNN_E_MODEL, "synapse generation: %s (%u)", what[rec[k].err], rec[k].err_arg);
     }
   // resolve the NormDev cache hand-off rank by rank, module by module

@@ -218,8 +218,23 @@ def cortical_grid(cfx: int, cfy: int, *, mu: float = 0.3, g_c: float = 3.0,
                   p1: Optional[float] = None, lam: float = 1.0,
                   total_ms: int = 1000, seed: int = 1, glob_h: int = 1,
                   stdp: bool = False, start_plasticity_ms: int = 0,
-                  delay_exponential: bool = False) -> NetConfig:
-    """The benchmark network family (see module docstring)."""
+                  delay_exponential: bool = False, delay_range_subpop: bool = False) -> NetConfig:
+    """The benchmark network family (see module docstring).
+
+    ``delay_range_subpop`` adds a fourth, empty sub-population (0 neurons, no
+    connection in or out) whose self-pair row declares DMax = 21 ms.  The
+    reference keeps the delay range of the whole problem as integers
+    (``delayMin``/``delayMax`` are uint32_t, DPSNN_parameters.h:111-112, set at
+    DPSNN_LIFCAconnectome.cpp:467-480) and splits it into 80 levels; with the
+    range 1-20 ms, getRandomDelay_UNI (DPSNN_LIFCAcorticalModuleGen.cpp:299-338)
+    maps the 60 largest of the 1e9 ran3 values to the float level 80.0 and
+    stops the run ("delay level generated ... max allowed delay levels"), so
+    the reference refuses any 1-20 ms network with more than a few tens of
+    millions of synapses (6x6 modules and up).  With the range 1-21 ms the
+    real pairs (DMin 1, DMax 20) use 76 levels of 0.25 ms: the same integer
+    delays 1-20 ms with the same weights (half-weight endpoints), and the
+    largest level is 76.0, so the reference builds every such network.
+    """
     if p1 is None:
         # 0.0376 at 2x2 reproduces the ~1125 in-degree of the 2x2 benchmark;
         # larger grids use the value giving the same grid-mean in-degree.
@@ -236,6 +251,13 @@ def cortical_grid(cfx: int, cfy: int, *, mu: float = 0.3, g_c: float = 3.0,
         J = mu if s < 2 else -4.0 * mu
         for t in range(3):
             conn[(s, t)] = (J, 0.1, 1.0, 20.0, probs)
+    if delay_range_subpop:
+        subpops.append(SubPop(0, **exc))
+        no_link = [0.0] * len(probs)
+        for s in range(4):
+            for t in range(4):
+                if s == 3 or t == 3:
+                    conn[(s, t)] = (mu, 0.1, 1.0, 21.0 if (s, t) == (3, 3) else 20.0, no_link)
     cfg = NetConfig(cfx=cfx, cfy=cfy, subpops=subpops, conn=conn,
                     stencil_dim=stencil_dim, total_ms=total_ms, seed=seed,
                     glob_h=glob_h, delay_exponential=delay_exponential)

@@ -171,10 +171,12 @@ void dpo_gaussian_lut(double mu, double sigma, double xmin, double xmax, double 
     for (int i = 0; i < 256; i++) table[i] = mu;
   }
 }
+/* erflib.c:172-181; a negative result wraps modulo 2^32 as in the
+ * reference's x86-64 build (truncation to 64 bits, low 32 bits kept). */
 uint32_t dpo_roundr2i(double r) {
   double i = floor(r);
-  if (i + 0.5 > r) return (uint32_t)i;
-  return (uint32_t)(i + 1.0);
+  if (i + 0.5 > r) return (uint32_t)(int64_t)i;
+  return (uint32_t)(int64_t)(i + 1.0);
 }
 
 /* ---------------------------------------------------------------- network */
@@ -292,7 +294,12 @@ static uint32_t random_delay_uni(dpo_net *n, o_rng *g, uint32_t s, uint32_t t) {
   DMin = dpo_roundr2i((DMin - DelayMin) / DelayStep) * DelayStep + DelayMin;
   outF = ((o_random(g) * (DMax - DMin) + DMin - DelayMin) / DelayStep);
   (void)DelayMax;
-  return dpo_roundr2i(outF * DelayStep);
+  if (outF >= DelayNum) return 0xFFFFFFFFu;   /* the reference's exit at :322-326 */
+  {
+    const uint32_t outfunc = dpo_roundr2i(outF * DelayStep);
+    if (outfunc > n->sp_DMax[s][t]) return 0xFFFFFFFFu;   /* :330-334 */
+    return outfunc;
+  }
 }
 
 /* getRandomDelay_EXP (DPSNN_LIFCAcorticalModuleGen.cpp:247-297): a truncated
@@ -395,7 +402,9 @@ static int generate(dpo_net *n, o_syn **gen_out, uint64_t **rank_gen_start_out) 
           if (dl == 0xFFFFFFFFu) { set_err("ERROR: delay level generated beyond the allowed delays"); return -1; }
           s.delay = (uint8_t)dl;
         } else {
-          s.delay = (uint8_t)random_delay_uni(n, g, ssub, tsub);
+          const uint32_t dl = random_delay_uni(n, g, ssub, tsub);
+          if (dl == 0xFFFFFFFFu) { set_err("ERROR: delay level generated beyond the allowed delays"); return -1; }
+          s.delay = (uint8_t)dl;
         }
         s.kind = (uint8_t)ssub;
         float mean = (float)n->sp_J[ssub][tsub];

@@ -20,11 +20,22 @@ built from the unmodified sources plus the bounds fix:
                           them),
                           spike and synaptic-event counts, configuration.
 
+* ``<case>.summary.npz`` for the networks of ``SUMMARY_CASES``, whose
+                          raster is too large to commit: per emission ms the
+                          spike count and CRC-32, per rank the raster's
+                          SHA-256 (see tests/golden/io.py); their manifest
+                          entry holds the BACKWARD dump SHA-256 of a few
+                          ranks and the per-population firing rates and ISI
+                          CV.  Those runs write the other ranks' synapse
+                          dumps to /dev/null.
+
 Usage: python tests/golden/make_golden.py [case ...]
 (with case names, only those entries of the manifest are regenerated)
 """
 import gzip
 import hashlib
+
+import numpy as np
 import importlib
 import io
 import json
@@ -37,7 +48,8 @@ import tempfile
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
-from tests.golden.cases import CASES  # noqa: E402
+from tests.golden.cases import CASES, SUMMARY_CASES  # noqa: E402
+from tests.golden import io as gio  # noqa: E402
 
 nc = importlib.import_module("201812realtimecortsim_b200.netconfig")
 REF_HP = os.path.join(ROOT, "oracle", "_ref", "dpsnn_ref_hp")
@@ -70,9 +82,14 @@ def gz_text(path):
     return io.TextIOWrapper(gzip.GzipFile(path, "wb", mtime=0))
 
 
-def run(binary, cfg, workdir):
+def run(binary, cfg, workdir, dump_ranks=None):
     env = dict(os.environ)
     env.update(cfg.write(workdir))
+    if dump_ranks is not None:   # the other ranks' synapse dumps are not kept
+        for h in range(cfg.glob_h):
+            if h not in dump_ranks:
+                os.symlink(os.devnull, os.path.join(
+                    workdir, f"localNet_h{h}_N{cfg.glob_n // cfg.glob_h}_SynapticList_BACKWARD_R-1.dat"))
     if cfg.delay_exponential:
         binary = {REF_HP: REF_EXP_HP, REF: REF_EXP}[binary]
     if cfg.glob_h > 1:   # one process per rank
@@ -81,6 +98,43 @@ def run(binary, cfg, workdir):
     r = subprocess.run([binary], cwd=workdir, env=env, capture_output=True, text=True)
     if r.returncode != 0 or "ERROR" in r.stdout:
         raise RuntimeError(r.stdout[-2000:] + r.stderr[-2000:])
+
+
+def read_raster(hp, cfg):
+    """The %.17g raster of every rank of a run, as (ids, times) arrays."""
+    ids, ts = [], []
+    for h in range(cfg.glob_h):
+        for sec in range((cfg.total_ms + 999) // 1000):
+            fn = os.path.join(hp, f"spikes-sec{sec}-C{cfg.n_modules}-H{cfg.glob_h}-h{h:03d}.dat")
+            if os.path.exists(fn):
+                a = np.loadtxt(fn, dtype=np.float64, ndmin=2)
+                if a.size:
+                    ids.append(a[:, 0].astype(np.uint32))
+                    ts.append(a[:, 1])
+    return np.concatenate(ids), np.concatenate(ts)
+
+
+def make_summary(name, manifest):
+    make, dump_ranks, (w0, w1) = SUMMARY_CASES[name]
+    cfg = make()
+    entry = {"total_ms": cfg.total_ms, "glob_h": cfg.glob_h, "glob_n": cfg.glob_n}
+    with tempfile.TemporaryDirectory(dir=os.environ.get("DPSNN_GOLDEN_TMP")) as td:
+        hp = os.path.join(td, "hp")
+        os.makedirs(hp)
+        run(REF_HP, cfg, hp, dump_ranks)
+        entry["backward_sha256"] = {}
+        for h in dump_ranks:
+            fn = f"localNet_h{h}_N{cfg.glob_n // cfg.glob_h}_SynapticList_BACKWARD_R-1.dat"
+            entry["backward_sha256"][str(h)] = sha256(os.path.join(hp, fn))
+        ids, ts = read_raster(hp, cfg)
+    cnt, crc = gio.per_ms_digests(ids, ts, cfg.total_ms)
+    rd = gio.rank_digests(ids, ts, cfg.glob_h, cfg.glob_n)
+    np.savez_compressed(os.path.join(HERE, f"{name}.summary.npz"), count_per_ms=cnt, crc_per_ms=crc,
+                        rank_sha256=rd)
+    rates, cvs = gio.pop_stats(ids, ts, [p.count for p in cfg.subpops], cfg.glob_n, w0, w1)
+    entry.update({"spikes": int(len(ids)), "stats_window_ms": [w0, w1], "rates_hz": rates, "isi_cv": cvs})
+    manifest[name] = entry
+    print(name, len(ids), "spikes", rates, cvs, flush=True)
 
 
 def main():
@@ -93,6 +147,9 @@ def main():
     if only:
         with open(os.path.join(HERE, "manifest.json")) as f:
             manifest = json.load(f)
+    for name in SUMMARY_CASES:
+        if only and name in only:
+            make_summary(name, manifest)
     for name, make in CASES.items():
         if only and name not in only:
             continue

@@ -43,9 +43,15 @@ def _env_for(cfg, workdir, monkeypatch):
         monkeypatch.setenv(k, v)
 
 
-@pytest.mark.parametrize("name", ["small_2x2", "small_2x2_stdp", "c1_2x2"])
+def _delay_range_grid():
+    from tests.conftest import netconfig
+    return netconfig().cortical_grid(6, 6, total_ms=100, glob_h=12, delay_range_subpop=True)
+
+
+@pytest.mark.parametrize("name", ["small_2x2", "small_2x2_stdp", "c1_2x2", "delay_range_6x6"])
 def test_parser_reads_what_netconfig_writes(name, tmp_path, monkeypatch):
-    cfg = CASES[name]()
+    # delay_range_6x6: a fourth, empty sub-population widening the delay range
+    cfg = _delay_range_grid() if name == "delay_range_6x6" else CASES[name]()
     _env_for(cfg, tmp_path, monkeypatch)
     got = E.params_from_env(str(tmp_path))
     want = E.params_from_netconfig(cfg)
