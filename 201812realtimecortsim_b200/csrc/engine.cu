@@ -1281,14 +1281,12 @@ __global__ void __launch_bounds__(NEURON_BLOCK) neuron_kernel(Dev d) {
 
 // Heavy neurons, more than LOCAL_EVENTS synaptic events in one step.
 // heavy_sort_kernel: one warp per neuron with at most HEAVY_WARP_MAX events
-// loads its bucket into shared memory, computes the arrival times,
+// loads its bucket into registers, computes the arrival times,
 // bitonic-sorts by (time, key) and writes the sorted events back into the
 // bucket; heavy_run_kernel then runs those neurons one thread each.  Neurons
 // with more events (including any beyond the bucket, in the overflow list)
 // are sorted and run by huge_kernel, one block each.
-#define HEAVY_WARP_MAX 256     // events a warp sorts in shared memory
-#define HEAVY_SORT_WARPS 4
-#define HEAVY_SORT_SMEM (HEAVY_SORT_WARPS * HEAVY_WARP_MAX * 16)
+#define HEAVY_WARP_MAX 256     // events a warp sorts in registers (8 per lane)
 #define HEAVY_MAX 8192
 #define HEAVY_THREADS 256
 #define HEAVY_SMEM (HEAVY_MAX * 16)
@@ -1326,73 +1324,126 @@ __device__ static inline uint32_t warp_path_max(const NetConst *net) {
   return min(net->ev_cap / 2, (uint32_t)HEAVY_WARP_MAX);
 }
 
-// The warp sort keeps times (8 B) and {key, weight} pairs (8 B, key in the
-// high half) in two shared arrays: a compare-exchange is four 8-byte loads
-// and at most four 8-byte stores (the kernel is bound by shared-memory
-// issue); equal times order by key, unique per target.
-__global__ void __launch_bounds__(HEAVY_SORT_WARPS * 32) heavy_sort_kernel(Dev d) {
-  extern __shared__ __align__(16) unsigned char hs_raw[];
+// Bitonic sort of 32*E events held in registers, E per lane: element
+// e = lane*E + r sits in register r of its lane.  An element is (arrival
+// time as IEEE bits, key, weight): times are positive, so their bit
+// patterns order like the times, and equal times order by key, which is
+// unique per target.  Exchanges between positions closer than E stay in the
+// lane's registers; the 15 farther ones (for E = 8) are one shuffle per
+// 32-bit word.  Ascending order at the end.
+template <int E>
+__device__ static inline void warp_sort_events(uint64_t (&tb)[E], uint32_t (&ky)[E], uint32_t (&wv)[E],
+                                               uint32_t lane) {
+#pragma unroll
+  for (int k = 2; k <= 32 * E; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j >= E) {
+        const int m = j / E;
+        const bool lower = (lane & (uint32_t)m) == 0;
+#pragma unroll
+        for (int r = 0; r < E; r++) {
+          const bool up = ((lane * E + r) & (uint32_t)k) == 0;
+          const uint32_t ylo = __shfl_xor_sync(0xffffffffu, (uint32_t)tb[r], m);
+          const uint32_t yhi = __shfl_xor_sync(0xffffffffu, (uint32_t)(tb[r] >> 32), m);
+          const uint32_t yk = __shfl_xor_sync(0xffffffffu, ky[r], m);
+          const uint32_t yw = __shfl_xor_sync(0xffffffffu, wv[r], m);
+          const uint64_t yt = ((uint64_t)yhi << 32) | ylo;
+          const bool x_lt_y = (tb[r] < yt) || (tb[r] == yt && ky[r] < yk);
+          // the lower position of an ascending pair keeps the smaller one
+          if ((lower == up) ? !x_lt_y : x_lt_y) {
+            tb[r] = yt;
+            ky[r] = yk;
+            wv[r] = yw;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < E; r++) {
+          if (r & j) continue;
+          const int q = r | j;
+          const bool up = ((lane * E + r) & (uint32_t)k) == 0;
+          const bool gt = (tb[r] > tb[q]) || (tb[r] == tb[q] && ky[r] > ky[q]);
+          if (gt == up) {
+            const uint64_t t0 = tb[r];
+            tb[r] = tb[q];
+            tb[q] = t0;
+            const uint32_t k0 = ky[r];
+            ky[r] = ky[q];
+            ky[q] = k0;
+            const uint32_t w0 = wv[r];
+            wv[r] = wv[q];
+            wv[q] = w0;
+          }
+        }
+      }
+    }
+  }
+}
+
+// One heavy neuron's n <= 32*E events: loaded with their arrival times,
+// sorted by (time, key) in registers, written back as sorted times into
+// the bucket's first half and weights into its second half.
+template <int E>
+__device__ static inline void heavy_sort_one(const Dev &d, uint2 *ev, uint32_t n, uint32_t t, uint32_t D,
+                                             uint32_t N, uint32_t cap, uint32_t lane) {
+  uint64_t tb[E];
+  uint32_t ky[E], wv[E];
+  uint2 x[E];
+#pragma unroll
+  for (int r = 0; r < E; r++) {
+    const uint32_t e = lane * E + r;
+    if (e < n) x[r] = ev[e];
+  }
+#pragma unroll
+  for (int r = 0; r < E; r++) {
+    const uint32_t e = lane * E + r;
+    if (e < n) {
+      tb[r] = (uint64_t)__double_as_longlong(event_time(d, x[r].x, t, D, N));
+      ky[r] = x[r].x;
+      wv[r] = x[r].y;
+    } else {   // padding after every event: +infinity, largest key
+      tb[r] = 0x7FF0000000000000ull;
+      ky[r] = 0xFFFFFFFFu;
+      wv[r] = 0u;
+    }
+  }
+  warp_sort_events<E>(tb, ky, wv, lane);
+  __syncwarp();   // every lane has read its events before the bucket is overwritten
+  double *st = reinterpret_cast<double *>(ev);
+  float *sv = reinterpret_cast<float *>(ev + cap / 2);
+#pragma unroll
+  for (int r = 0; r < E; r++) {
+    const uint32_t e = lane * E + r;
+    if (e < n) {
+      st[e] = __longlong_as_double((long long)tb[r]);
+      sv[e] = __uint_as_float(wv[r]);
+    }
+  }
+}
+
+#define HEAVY_SORT_THREADS 256
+
+// A warp per neuron of the warp path (LOCAL_EVENTS < n <= HEAVY_WARP_MAX):
+// registers only, no shared memory.
+__global__ void __launch_bounds__(HEAVY_SORT_THREADS, 4) heavy_sort_kernel(Dev d) {
   const NetConst *net = d.net;
   const uint32_t t = *d.t, N = net->N, D = net->D, cap = net->ev_cap, wmax = warp_path_max(net);
-  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  double *tau = reinterpret_cast<double *>(hs_raw) + (size_t)w * HEAVY_WARP_MAX;
-  unsigned long long *kv =
-      reinterpret_cast<unsigned long long *>(hs_raw + (size_t)HEAVY_SORT_WARPS * HEAVY_WARP_MAX * 8) +
-      (size_t)w * HEAVY_WARP_MAX;
+  const uint32_t lane = threadIdx.x & 31;
   const uint32_t nh = min(d.heavy_cnt[0], N);
-  for (uint32_t hh = blockIdx.x * HEAVY_SORT_WARPS + w; hh < nh; hh += gridDim.x * HEAVY_SORT_WARPS) {
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t hh = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; hh < nh; hh += nwarps) {
     const uint32_t i = d.heavy_list[hh], n = d.heavy_list[N + hh];
     if (n > wmax) continue;   // not listed here
     uint2 *ev = d.ev + (size_t)i * cap;
-    uint32_t n2 = 1;
-    while (n2 < n) n2 <<= 1;
-    // the bucket's events and their arrival times, 4 per lane in flight
-    for (uint32_t e0 = 0; e0 < n2; e0 += 128) {
-      uint2 x[4];
-#pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const uint32_t e = e0 + 32 * u + lane;
-        if (e < n) x[u] = ev[e];
-      }
-#pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const uint32_t e = e0 + 32 * u + lane;
-        if (e < n) {
-          tau[e] = event_time(d, x[u].x, t, D, N);
-          kv[e] = ((unsigned long long)x[u].x << 32) | x[u].y;
-        } else if (e < n2) {
-          tau[e] = INFINITY;
-          kv[e] = ~0ull;
-        }
-      }
-    }
-    __syncwarp();
-    for (uint32_t k = 2; k <= n2; k <<= 1) {
-      for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-        // pair p compares a = p with bit j inserted as 0, and b = a | j
-        for (uint32_t p = lane; p < (n2 >> 1); p += 32) {
-          const uint32_t a = ((p & ~(j - 1)) << 1) | (p & (j - 1)), b = a | j;
-          const double ta = tau[a], tb = tau[b];
-          const unsigned long long ka = kv[a], kb = kv[b];
-          const bool gt = (ta > tb) || (ta == tb && ka > kb);
-          if (gt == ((a & k) == 0)) {
-            tau[a] = tb;
-            tau[b] = ta;
-            kv[a] = kb;
-            kv[b] = ka;
-          }
-        }
-        __syncwarp();
-      }
-    }
-    // sorted arrival times into the bucket's first half, weights into its second
-    double *st = reinterpret_cast<double *>(ev);
-    float *sv = reinterpret_cast<float *>(ev + cap / 2);
-    for (uint32_t e = lane; e < n; e += 32) {
-      st[e] = tau[e];
-      sv[e] = __uint_as_float((uint32_t)kv[e]);
-    }
-    __syncwarp();
+    if (n <= 32)
+      heavy_sort_one<1>(d, ev, n, t, D, N, cap, lane);
+    else if (n <= 64)
+      heavy_sort_one<2>(d, ev, n, t, D, N, cap, lane);
+    else if (n <= 128)
+      heavy_sort_one<4>(d, ev, n, t, D, N, cap, lane);
+    else
+      heavy_sort_one<8>(d, ev, n, t, D, N, cap, lane);
   }
 }
 
@@ -2165,12 +2216,11 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
   e->grid_deliver = (uint32_t)sms * 8;
-  e->grid_heavy = (uint32_t)sms * 14;      // 16 KB of shared memory per block
+  e->grid_heavy = (uint32_t)sms * 8;
   e->grid_heavy_run = (uint32_t)sms * 16;
   e->grid_huge = (uint32_t)sms;
   CK(cudaFuncSetAttribute(bath_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(BathSmem)));
   CK(cudaFuncSetAttribute(huge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, HEAVY_SMEM));
-  CK(cudaFuncSetAttribute(heavy_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, HEAVY_SORT_SMEM));
   CK(cudaStreamSynchronize(e->stream));
   return 0;
 }
@@ -2357,7 +2407,7 @@ static int enqueue_step(dpsnn_engine *e) {
   neuron_kernel<<<e->grid_neuron, NEURON_BLOCK, 0, e->stream>>>(d);
   timed_launch_end(e, 3);
   timed_launch_begin(e, 5);
-  heavy_sort_kernel<<<e->grid_heavy, HEAVY_SORT_WARPS * 32, HEAVY_SORT_SMEM, e->stream>>>(d);
+  heavy_sort_kernel<<<e->grid_heavy, HEAVY_SORT_THREADS, 0, e->stream>>>(d);
   timed_launch_end(e, 5);
   timed_launch_begin(e, 6);
   heavy_run_kernel<<<e->grid_heavy_run, 128, 0, e->stream>>>(d);

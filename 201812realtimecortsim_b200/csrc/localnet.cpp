@@ -315,6 +315,13 @@ uint32_t env_u32_or(const char *name, uint32_t dflt) {
 
 }  // namespace
 
+dpsnn_params getParameters(const uint32_t loc_h) {
+  (void)loc_h;
+  dpsnn_params par;
+  if (dpsnn_params_from_env(nullptr, &par)) die("getParameters");
+  return par;
+}
+
 void localNetProcess_init(DALProcess *p) {
   (void)p;
   if (g_net) {

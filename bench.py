@@ -18,11 +18,10 @@ e2e    = the same metric through the C ABI as a drop-in caller uses it: one
 modules, --batch-ms biological ms of each, stepped together (dpsnn_step_many)
 and, on freshly built engines, one after another (dpsnn_step), printing one
 JSON line with both aggregate rates.
-The reference arm (--impl reference) runs the reference binary built from the
-reference sources (oracle/_ref/dpsnn_ref) on the host cores: one single-rank
-process per core, each simulating the 2x2 network (the reference's
-CPU-runnable case: 5000 neurons, ~5.6 M synapses, 1 s), events counted by the
-committed fixture of that run.
+The reference arm (--impl reference) runs the reference built from its
+sources on the same network and steps as the engine's timed region, as 192
+MPI processes (a forked shared-memory MPI subset, oracle/mpi_shm) on the
+host cores, timed by its own per-step chrono over steps W..W+K-1.
 """
 from __future__ import annotations
 
@@ -158,52 +157,135 @@ def reference_events_c1() -> int:
         return int(json.load(f)["c1_2x2"]["events"])
 
 
-def reference_processes() -> int:
-    """One reference process per host thread, bounded by host memory
-    (about 0.4 GB resident per process)."""
-    n = os.cpu_count() or 1
-    if os.environ.get("DPSNN_BENCH_REF_PROCS"):   # a smaller sample (tests)
-        n = max(1, int(os.environ["DPSNN_BENCH_REF_PROCS"]))
-    try:
-        import psutil
-        n = min(n, max(1, int(psutil.virtual_memory().available / 1.0e9)))
-    except Exception:
-        pass
-    return n
+def bench_network(args):
+    """The benchmark network (netconfig) and its workload name.  The grid
+    carries the empty delay-range sub-population, without which the
+    reference refuses networks of this size (netconfig.cortical_grid)."""
+    nc = importlib.import_module("201812realtimecortsim_b200.netconfig")
+    cfx, cfy = (int(x) for x in args.grid.lower().split("x"))
+    total_ms = max(args.full_ms, args.warmup + args.steps + 10)
+    cfg = nc.cortical_grid(cfx, cfy, total_ms=total_ms, glob_h=args.ranks, delay_range_subpop=True)
+    workload = WORKLOAD if (cfx, cfy, args.ranks) == (24, 24, 192) else (
+        f"{cfx}x{cfy} grid, {cfg.glob_n} neurons, 1 ms steps, STDP off, RNG streams of {args.ranks} ranks")
+    return cfg, workload
+
+
+PARTIAL_RE = re.compile(r"PartialTimeStep = ([0-9.eE+-]+)")
+REF_CASE = "c2_24x24_p192"   # reference-derived events per step of the benchmark network
+
+
+def reference_window(cfg, binary, workdir, W, K, raster):
+    """Run the reference (env_globH processes over oracle/mpi_shm) for W+K
+    steps of ``cfg`` in ``workdir``; return the seconds its own
+    PartialTimeStep chrono (DPSNN_localNet_sim.c:59,305) measured over steps
+    W..W+K-1, the slowest rank's.  Without ``raster`` its spike and rate
+    files are off (its fastest stock configuration); its synapse-list dump
+    goes to /dev/null."""
+    os.makedirs(workdir, exist_ok=True)
+    env = dict(os.environ)
+    env.update(cfg.write(workdir))
+    env["env_totalSimTime_ms"] = str(W + K)
+    env["env_startPartialChrono_ms"] = str(W)
+    env["env_partialChronoWindow_ms"] = str(K)
+    if not raster:
+        env["env_spikes_writeDisable"] = "1"
+        env["env_statRatesPerPop_writeDisable"] = "1"
+    env["DPSNN_SHM_RANKS"] = str(cfg.glob_h)
+    os.symlink(os.devnull, os.path.join(
+        workdir, f"localNet_h0_N{cfg.glob_n // cfg.glob_h}_SynapticList_BACKWARD_R-1.dat"))
+    r = subprocess.run([binary], cwd=workdir, env=env, capture_output=True, text=True)
+    if r.returncode != 0 or "ERROR" in r.stdout:
+        raise RuntimeError("reference run failed: " + (r.stdout[-500:] + r.stderr[-500:]).strip())
+    secs = []
+    for h in range(cfg.glob_h):
+        with open(os.path.join(workdir, f"SummaryStatMeasures_h{h}.stat")) as f:
+            m = PARTIAL_RE.search(f.read())
+        if not m:
+            raise RuntimeError(f"rank {h} reported no PartialTimeStep")
+        secs.append(float(m.group(1)))
+    return max(secs)
+
+
+def reference_window_events(cfg, W, K, workdir):
+    """Synaptic events of steps W..W+K-1 (addInputSpike calls; the reference
+    prints no count): the committed reference-derived counts of the
+    benchmark network, else those of an untimed full-precision reference run
+    over the restatement's out-degree per (neuron, delay)."""
+    man = os.path.join(ROOT, "tests", "golden", "manifest.json")
+    npz = os.path.join(ROOT, "tests", "golden", f"{REF_CASE}.summary.npz")
+    if os.path.exists(npz):
+        sys.path.insert(0, ROOT)
+        from tests.golden.cases import SUMMARY_CASES
+        ref_cfg = SUMMARY_CASES[REF_CASE][0]()
+        same = (ref_cfg.env() | {"env_totalSimTime_ms": "", "env_partialChronoWindow_ms": ""}) == \
+               (cfg.env() | {"env_totalSimTime_ms": "", "env_partialChronoWindow_ms": ""}) and \
+               ref_cfg.column_txt() == cfg.column_txt() and ref_cfg.connectivity_txt() == cfg.connectivity_txt()
+        import numpy as np
+        ev = []
+        if same:
+            with np.load(npz) as z:
+                ev = z["events_per_step"]
+        if same and W + K <= len(ev):
+            return int(ev[W:W + K].sum()), "reference raster of the benchmark network (tests/golden), " \
+                                            "restatement out-degree"
+    binary = os.path.join(ROOT, "oracle", "_ref", "dpsnn_ref_mp_hp" if cfg.glob_h > 1 else "dpsnn_ref_hp")
+    reference_window(cfg, binary, workdir, W, K, raster=True)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import dpsnn_oracle as O
+    import numpy as np
+    ids, ts = [], []
+    for h in range(cfg.glob_h):
+        fn = os.path.join(workdir, f"spikes-sec0-C{cfg.n_modules}-H{cfg.glob_h}-h{h:03d}.dat")
+        if os.path.exists(fn) and os.path.getsize(fn):
+            a = np.loadtxt(fn, ndmin=2)
+            ids.append(a[:, 0].astype(np.int64))
+            ts.append(a[:, 1])
+    ids = np.concatenate(ids) if ids else np.zeros(0, np.int64)
+    ts = np.concatenate(ts) if ts else np.zeros(0)
+    ev = O.events_per_step(O.outdegree_by_delay(cfg), ids, ts, W + K)
+    return int(ev[W:W + K].sum()), "untimed full-precision reference run, restatement out-degree"
 
 
 def run_reference(args, world, rank):
-    """Reference arm: the reference binary built from its sources, one
-    single-rank process per host thread, each simulating 1000 ms of the 2x2
-    grid; a bench step is one such batch (at most 2 batches are timed)."""
+    """Reference arm: the reference built from its sources, on the same
+    network and steps as the engine's timed region (steps W..W+K-1), run as
+    env_globH MPI processes (oracle/mpi_shm: forked processes over shared
+    memory) on the host cores; time = its own PartialTimeStep chrono over
+    those steps."""
     if rank != 0:
         return
-    binary = os.path.join(ROOT, "oracle", "_ref", "dpsnn_ref")
+    cfg, workload = bench_network(args)
+    W, K = args.warmup, args.steps
+    binary = os.path.join(ROOT, "oracle", "_ref", "dpsnn_ref_mp" if cfg.glob_h > 1 else "dpsnn_ref")
     if not os.path.exists(binary):
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/dpsnn_ref was not built"}))
+        print(json.dumps({"impl": "reference", "unavailable": f"{os.path.relpath(binary, ROOT)} was not built"}))
         return
-    cores = reference_processes()
-    events = reference_events_c1()
-    batches = max(1, min(args.steps, 2))
-    rates, walls = [], []
-    for it in range(batches):
-        with tempfile.TemporaryDirectory() as td:
-            t0 = time.perf_counter()
-            procs = [reference_c1_start(os.path.join(td, f"r{c}"), binary) for c in range(cores)]
-            fire = [reference_fire_seconds(p) for p in procs]
-            walls.append(time.perf_counter() - t0)
-        rates.append(sum(events / f for f in fire))
-    value = statistics.mean(rates)
-    sample = (f"reference binary, 2x2 grid (5000 neurons, 5.6M synapses), 1000 ms per process, "
-              f"{cores} concurrent processes, {batches} batch(es); time = its own fire() CHRONO")
+    need_gb = 0.3 * cfg.glob_h * (cfg.glob_n / cfg.glob_h) / 3750.0   # ~0.21 GB per rank of 3750 neurons
+    try:
+        import psutil
+        avail_gb = psutil.virtual_memory().available / 1e9
+    except Exception:
+        avail_gb = need_gb
+    if avail_gb < need_gb:
+        print(json.dumps({"impl": "reference", "unavailable": f"{cfg.glob_h} reference processes need "
+                          f"~{need_gb:.0f} GB of host memory, {avail_gb:.0f} GB available"}))
+        return
+    with tempfile.TemporaryDirectory() as td:
+        secs = reference_window(cfg, binary, os.path.join(td, "timed"), W, K, raster=False)
+        events, how = reference_window_events(cfg, W, K, os.path.join(td, "events"))
+    value = events / secs
+    cores = min(cfg.glob_h, os.cpu_count() or 1)   # one process per rank, at most one per host thread busy
+    sample = (f"reference built from its sources, {workload}, steps {W}-{W + K - 1}, {cfg.glob_h} MPI "
+              f"processes on {cores} host threads, spike and rate files off; time = its PartialTimeStep "
+              f"chrono (slowest rank), {secs:.3f} s; events: {how}")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": batches, "warmup": 0, "ms_per_step": 1e3 * statistics.mean(walls),
+        "steps": K, "warmup": W, "ms_per_step": 1e3 * secs / K,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic: network generated by the reference's own generator, seed 1",
-        "config": {"workload": "2x2 grid, 5000 neurons, 1 ms steps, STDP off, 1 rank per process "
-                               "(the reference's CPU-runnable case; the 24x24 grid needs 192 MPI ranks)",
-                   "parallelism": f"{cores} processes"},
+        "config": {"workload": workload, "parallelism": f"{cfg.glob_h} MPI processes",
+                   "real_time_factor": secs / (K * 1e-3), "events_per_step": events / K,
+                   "timed_steps": [W, W + K - 1]},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
@@ -290,6 +372,8 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--e2e-steps", type=int, default=0, help="0 = the same K steps as the timed region")
+    ap.add_argument("--full-ms", type=int, default=10000,
+                    help="steps of the whole run timed for full_run (the network's biological ms; 0 = skip)")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", default="24x24", help="CFXxCFY modules (profiling of smaller grids)")
@@ -312,19 +396,9 @@ def main():
 
     import torch
     E = importlib.import_module("201812realtimecortsim_b200.engine")
-    nc = importlib.import_module("201812realtimecortsim_b200.netconfig")
     torch.cuda.set_device(local)
-    prof_steps = min(200, args.steps)
-    total_ms = max(10000, args.warmup + args.steps + prof_steps + args.e2e_steps + 10)
-    cfx, cfy = (int(x) for x in args.grid.lower().split("x"))
-    cfg = nc.cortical_grid(cfx, cfy, total_ms=total_ms, glob_h=args.ranks)
-    workload = WORKLOAD if (cfx, cfy, args.ranks) == (24, 24, 192) else (
-        f"{cfx}x{cfy} grid, {cfg.glob_n} neurons, 1 ms steps, STDP off, RNG streams of {args.ranks} ranks")
-    eng = E.Engine(cfg, device=local)
-    eng_bytes = 6 * eng.synapse_count
-    eng.step(args.warmup)
-    eng.sync()
-    stream = torch.cuda.ExternalStream(eng.cuda_stream())
+    cfg, workload = bench_network(args)
+    total_ms = cfg.total_ms
 
     def all_max(x):
         if not dist:
@@ -340,41 +414,69 @@ def main():
         dist.all_reduce(t)
         return float(t.item())
 
-    # timed region: K steps, device time on the engine stream
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    def device_seconds(eng, stream, n):
+        """Device time of n steps on the engine stream (CUDA events)."""
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        eng.step(n)
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b) * 1e-3
+
+    # 1. timed region: steps W .. W+K-1, device time on the engine stream
+    eng = E.Engine(cfg, device=local)
+    eng_bytes = 6 * eng.synapse_count
+    stream = torch.cuda.ExternalStream(eng.cuda_stream())
+    warm_s = device_seconds(eng, stream, args.warmup)
+    eng.sync()
     e0 = eng.events_delivered()
     l0 = eng.kernel_launches()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
-        ev0.record(stream)
-        eng.step(args.steps)
-        ev1.record(stream)
-        ev1.synchronize()
+        elapsed = device_seconds(eng, stream, args.steps)
     torch.cuda.synchronize()
     eng.sync()
-    elapsed = ev0.elapsed_time(ev1) * 1e-3
     events = eng.events_delivered() - e0
     launches = eng.kernel_launches() - l0
     t_max = all_max(elapsed)
     ev_tot = all_sum(events)
 
-    # per-kernel-family device times over the following steps (event pairs
-    # around each family; kept out of the timed region above)
-    eng.set_timing(True)
+    # 2. the whole run the metric is quoted on (the network's total_ms steps,
+    # 10 s by default): the same engine continues; device time of its three
+    # segments (warm-up, timed region, the rest)
+    full = None
+    rest = total_ms - args.warmup - args.steps
+    if args.full_ms and rest > 0:
+        with ClockSampler(local) as clk_full:
+            rest_s = device_seconds(eng, stream, rest)
+        eng.sync()
+        full_s = all_max(warm_s + elapsed + rest_s)
+        full_ev = all_sum(eng.events_delivered())
+        full = {"steps": total_ms, "seconds": full_s, "real_time_factor": full_s / (total_ms * 1e-3),
+                "value": full_ev / full_s, "unit": UNIT, "events_per_step": full_ev / world / total_ms,
+                "clocks": clk_full.summary()}
+    eng.close()
+
+    # 3. per-kernel-family device times on an identical replay of steps
+    # W .. W+K-1 (the simulation is deterministic: same network, same
+    # steps); event pairs around each family, kept out of the timed region
+    eng = E.Engine(cfg, device=local)
+    eng.step(args.warmup)
+    eng.sync()
     p0 = eng.events_delivered()
-    eng.step(prof_steps)
+    eng.set_timing(True)
+    eng.step(args.steps)
     eng.sync()
     eng.set_timing(False)
     ksec, kcnt = eng.kernel_times()
     prof_events = eng.events_delivered() - p0
-
     eng.close()
 
-    # e2e: the same steps W..W+K-1 of the same network (the simulation is
-    # deterministic), stepped one at a time through the C ABI with each
-    # step's spike list read back to host memory, timed on the host
+    # 4. e2e: the same steps W..W+K-1 of the same network, stepped one at a
+    # time through the C ABI with each step's spike list read back to host
+    # memory, timed on the host
     eng = E.Engine(cfg, device=local)
     eng.step(args.warmup)
     eng.sync()
@@ -398,7 +500,7 @@ def main():
     fam = E.TIMING_NAMES
     fam_total = float(sum(ksec)) or 1.0
     kernel_share = {f: float(s) / fam_total for f, s in zip(fam, ksec)}
-    kernel_ms = {f: (1e3 * float(s) / prof_steps) for f, s in zip(fam, ksec)}   # per step
+    kernel_ms = {f: (1e3 * float(s) / args.steps) for f, s in zip(fam, ksec)}   # per step
     # delivery kernel: per synaptic event it reads the u32 target and the
     # i16 weight of the synapse and writes one 8-byte {key, weight} record
     deliver_s = float(ksec[1]) / max(int(kcnt[1]), 1)
@@ -429,13 +531,17 @@ def main():
                        "parallelism": f"replicas x{world}",
                        "l2": f"inputs larger than L2 (connectome {eng_bytes / 1e9:.1f} GB of CSR read every step)",
                        "real_time_factor": t_max / (args.steps * 1e-3),
-                       "events_per_step": events / args.steps},
+                       "events_per_step": events / args.steps,
+                       "timed_steps": [args.warmup, args.warmup + args.steps - 1]},
             "roofline": {"bound": "hbm", "kernel": "deliver_kernel", "achieved": achieved, "peak": hbm,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": traffic, "algorithmic_bytes_per_event": 14,
                          "events_per_launch": ev_per_launch},
             "kernel_ms_per_step": kernel_ms,
             "kernel_share": kernel_share,
+            "kernel_replay": {"steps": [args.warmup, args.warmup + args.steps - 1],
+                              "events_identical_to_timed": prof_events == events},
+            "full_run": full,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": d2h / max(e2e_steps, 1), "steps": e2e_steps,
                     "ms_per_step": 1e3 * (h1 - h0) / max(e2e_steps, 1)},
@@ -444,11 +550,9 @@ def main():
             "cpu_baseline": cpu,
         }
         print(json.dumps(out))
-    eng.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
-
 
 if __name__ == "__main__":
     main()

@@ -34,6 +34,9 @@
 #ifndef DPSNN_LOCALNET_H
 #define DPSNN_LOCALNET_H
 
+#include <stdint.h>
+#include "dpsnn_b200.h"
+
 #ifndef DAL_H
 /* The process handle of the reference's dal.h:24-42, same layout and tag. */
 typedef struct _local_states *LocalState;
@@ -59,6 +62,17 @@ void localNetProcess_finish(DALProcess *p);
 /* Handle of the engine the trio drives (NULL before init / after finish),
  * for callers that also want the C ABI of dpsnn_b200.h. */
 struct dpsnn_engine *localNetProcess_engine(void);
+
+/* getParameters (DPSNN_getParameters.c:23-831, declared at
+ * DPSNN_getParameters.h:7 with C++ linkage): the run's parameters from the
+ * env_* variables and the input files of the current directory, by the
+ * reference's rules; on an error it prints "ERROR ..." and exits with status
+ * 0, as the reference does.  loc_h is accepted for the signature's sake: every
+ * rank of a run reads the same parameters (the rank number only selects the
+ * emulated rank's output files).  The result is the engine's parameter
+ * block (dpsnn_b200.h), not the reference's struct DPSNN_parameters: a
+ * caller compiled against the reference's header must not call this one. */
+dpsnn_params getParameters(const uint32_t loc_h);
 #endif
 
 #endif

@@ -333,10 +333,12 @@ static uint32_t random_delay_exp(dpo_net *n, o_rng *g, uint32_t s, uint32_t t) {
 
 typedef struct { uint32_t glob, host, sub; } o_target;
 
-static int generate(dpo_net *n, o_syn **gen_out, uint64_t **rank_gen_start_out) {
+static int generate(dpo_net *n, o_syn **gen_out, uint64_t **rank_gen_start_out, uint16_t *outdeg) {
   /* Returns all generated synapses in generation order (rank-major, since
-   * each rank walks its own neurons) plus per-rank start offsets. */
-  uint64_t cap = 1u << 20, cnt = 0;
+   * each rank walks its own neurons) plus per-rank start offsets.  With
+   * outdeg (count-only mode) nothing is stored: outdeg[pre * D + delay]
+   * counts the synapses instead. */
+  uint64_t cap = outdeg ? 1 : (1u << 20), cnt = 0;
   o_syn *gen = malloc(cap * sizeof *gen);
   uint64_t *rstart = calloc(n->glob_h + 1, sizeof *rstart);
   o_target *tl = malloc(sizeof(o_target) * 8192 * 4);
@@ -395,7 +397,7 @@ static int generate(dpo_net *n, o_syn **gen_out, uint64_t **rank_gen_start_out) 
         memset(&s, 0, sizeof s);
         s.pre = gn;
         s.post = tl[j].glob;
-        n->fwd_hosts[(size_t)gn * n->glob_h + tl[j].host]++;
+        if (!outdeg) n->fwd_hosts[(size_t)gn * n->glob_h + tl[j].host]++;
         uint32_t tsub = tl[j].sub;
         if (n->cfg.delay_exp) {
           const uint32_t dl = random_delay_exp(n, g, ssub, tsub);
@@ -420,6 +422,10 @@ static int generate(dpo_net *n, o_syn **gen_out, uint64_t **rank_gen_start_out) 
           return -1;
         }
         s.weight = (int16_t)(wf * n->f2w);
+        if (outdeg) {
+          outdeg[(size_t)gn * n->D + s.delay]++;
+          continue;
+        }
         if (cnt == cap) {
           cap *= 2;
           gen = realloc(gen, cap * sizeof *gen);
@@ -446,6 +452,11 @@ static int generate(dpo_net *n, o_syn **gen_out, uint64_t **rank_gen_start_out) 
   }
   rstart[n->glob_h] = cnt;
   free(tl);
+  if (outdeg) {
+    free(gen);
+    free(rstart);
+    return 0;
+  }
   *gen_out = gen;
   *rank_gen_start_out = rstart;
   return 0;
@@ -537,17 +548,16 @@ static int build_rank(dpo_net *n, uint32_t hp, const o_syn *gen, const uint64_t 
   return 0;
 }
 
-dpo_net *dpo_create(const dpo_config *cfg, int libm_mode) {
-  g_libm_mode = libm_mode;
-  dpo_net *n = calloc(1, sizeof *n);
-  if (!n) return NULL;
+/* The configuration-derived tables of a network (sizes, sub-population
+ * parameters, delay range, mirrored stencil probabilities, bath LUTs, STDP
+ * tables); 0 on success. */
+static int net_params(dpo_net *n, const dpo_config *cfg) {
   n->cfg = *cfg;
   n->nsub = cfg->nsub;
   if (n->nsub == 0 || n->nsub > DPO_MAX_SUB || cfg->stencil_dim == 0 ||
       cfg->stencil_dim > DPO_MAX_STENCIL || cfg->glob_h == 0 || cfg->D == 0 || cfg->D > O_RING) {
     set_err("configuration out of range");
-    free(n);
-    return NULL;
+    return -1;
   }
   n->npcm = 0;
   for (uint32_t s = 0; s < n->nsub; s++) {
@@ -557,8 +567,7 @@ dpo_net *dpo_create(const dpo_config *cfg, int libm_mode) {
   n->glob_cft = cfg->cfx * cfg->cfy;
   if ((n->glob_cft % cfg->glob_h) != 0) {
     set_err("globCFT must be a multiple of globH");
-    free(n);
-    return NULL;
+    return -1;
   }
   float loc_cft = (float)n->glob_cft / (float)cfg->glob_h;
   n->loc_n = (uint32_t)(n->npcm * loc_cft);
@@ -617,7 +626,12 @@ dpo_net *dpo_create(const dpo_config *cfg, int libm_mode) {
   n->anti_tab[0] = cfg->stdp_antiCausalCoeff * cfg->stdp_antiCausalMax * cfg->stdp_multiplier;
   for (int i = 1; i < 128; i++) n->causal_tab[i] = (1 - 1 / cfg->stdp_tau_ms) * n->causal_tab[i - 1];
   for (int i = 1; i < 128; i++) n->anti_tab[i] = (1 - 1 / cfg->stdp_tau_ms) * n->anti_tab[i - 1];
+  return 0;
+}
 
+/* Per-neuron arrays that generation writes (state initialisation, bath
+ * parameters) and the per-rank RNG holders. */
+static int net_neuron_arrays(dpo_net *n) {
   size_t N = n->glob_n;
   n->v = calloc(N, sizeof(double));
   n->c = calloc(N, sizeof(double));
@@ -628,9 +642,42 @@ dpo_net *dpo_create(const dpo_config *cfg, int libm_mode) {
   n->max_ext = calloc(N, sizeof(uint32_t));
   n->sub = calloc(N, 1);
   n->fired = calloc(N, 1);
+  n->rank = calloc(n->glob_h, sizeof(o_rank));
+  if (!n->v || !n->c || !n->tr || !n->te || !n->nb || !n->inv_nu || !n->max_ext || !n->sub || !n->fired ||
+      !n->rank) {
+    set_err("out of memory");
+    return -1;
+  }
+  return 0;
+}
+
+int dpo_outdegree_by_delay(const dpo_config *cfg, int libm_mode, uint16_t *out) {
+  /* Synapses per (presynaptic neuron, delay slot), out[pre * D + delay],
+   * from the generation alone (no synapse lists, no delay rings). */
+  g_libm_mode = libm_mode;
+  dpo_net *n = calloc(1, sizeof *n);
+  if (!n) return -1;
+  int rc = net_params(n, cfg);
+  if (rc == 0) rc = net_neuron_arrays(n);
+  if (rc == 0) {
+    memset(out, 0, (size_t)n->glob_n * n->D * sizeof(uint16_t));
+    rc = generate(n, NULL, NULL, out);
+  }
+  dpo_destroy(n);
+  return rc;
+}
+
+dpo_net *dpo_create(const dpo_config *cfg, int libm_mode) {
+  g_libm_mode = libm_mode;
+  dpo_net *n = calloc(1, sizeof *n);
+  if (!n) return NULL;
+  if (net_params(n, cfg) != 0 || net_neuron_arrays(n) != 0) {
+    dpo_destroy(n);
+    return NULL;
+  }
+  size_t N = n->glob_n;
   n->last_spike_ms = calloc(N, sizeof(int32_t));
   n->fwd_hosts = calloc(N * n->glob_h, sizeof(uint32_t));
-  n->rank = calloc(n->glob_h, sizeof(o_rank));
   n->spk_ids = malloc(N * sizeof(uint32_t));
   n->spk_t = malloc(N * sizeof(double));
   n->rank_spk_start = calloc(n->glob_h + 1, sizeof(uint32_t));
@@ -644,7 +691,7 @@ dpo_net *dpo_create(const dpo_config *cfg, int libm_mode) {
   for (size_t i = 0; i < N; i++) n->last_spike_ms[i] = -100000;
   o_syn *gen = NULL;
   uint64_t *rstart = NULL;
-  if (generate(n, &gen, &rstart) != 0) { dpo_destroy(n); return NULL; }
+  if (generate(n, &gen, &rstart, NULL) != 0) { dpo_destroy(n); return NULL; }
   for (uint32_t h = 0; h < n->glob_h; h++)
     if (build_rank(n, h, gen, rstart) != 0) { free(gen); free(rstart); dpo_destroy(n); return NULL; }
   free(gen);

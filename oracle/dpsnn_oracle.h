@@ -72,6 +72,10 @@ enum { DPO_LIBM_SYSTEM = 0, DPO_LIBM_CORRECTLY_ROUNDED = 1 };
 
 dpo_net *dpo_create(const dpo_config *cfg, int libm_mode);
 void dpo_destroy(dpo_net *n);
+/* Synapses per (presynaptic neuron, delay slot), out[pre * D + delay]
+ * (glob_n * D entries), by the generation alone: no synapse lists or delay
+ * rings are built, so any network size fits.  0 on success. */
+int dpo_outdegree_by_delay(const dpo_config *cfg, int libm_mode, uint16_t *out);
 const char *dpo_last_error(void);
 
 uint32_t dpo_glob_n(const dpo_net *n);

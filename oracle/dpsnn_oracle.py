@@ -53,6 +53,7 @@ def _lib():
     lib.dpo_create.restype = P
     lib.dpo_create.argtypes = [C.POINTER(DpoConfig), C.c_int]
     lib.dpo_destroy.argtypes = [P]
+    lib.dpo_outdegree_by_delay.argtypes = [C.POINTER(DpoConfig), C.c_int, P]
     lib.dpo_last_error.restype = C.c_char_p
     for name in ("dpo_glob_n", "dpo_loc_n", "dpo_time_ms"):
         getattr(lib, name).restype = C.c_uint32
@@ -130,6 +131,29 @@ def config_from_netconfig(cfg) -> DpoConfig:
     c.stdp_tauDecay_s, c.stdp_drift = tdec, drift
     c.delay_exp = 1 if getattr(cfg, "delay_exponential", False) else 0
     return c
+
+
+def outdegree_by_delay(cfg, libm_mode: int = 0) -> np.ndarray:
+    """(glob_n, D) uint16: synapses of each presynaptic neuron per delay slot,
+    from the restatement's generation alone (any network size)."""
+    c = config_from_netconfig(cfg)
+    out = np.zeros((cfg.glob_n, cfg.D), np.uint16)
+    if lib().dpo_outdegree_by_delay(C.byref(c), libm_mode, _ptr(out)) != 0:
+        raise RuntimeError("oracle: " + lib().dpo_last_error().decode())
+    return out
+
+
+def events_per_step(outdeg: np.ndarray, ids: np.ndarray, ts: np.ndarray, total_ms: int) -> np.ndarray:
+    """Synaptic events delivered at each step 0..total_ms-1 by the spikes of a
+    raster: a spike emitted during ms m is compacted at step m+1 and its
+    synapses of delay slot d are delivered at step m+1+d
+    (DPSNN_localNet_sim.c:837-999)."""
+    D = outdeg.shape[1]
+    ev = np.zeros(total_ms + D + 1, np.int64)
+    step0 = np.floor(ts).astype(np.int64) + 1
+    for d in range(D):
+        np.add.at(ev, step0 + d, outdeg[ids, d].astype(np.int64))
+    return ev[:total_ms]
 
 
 class OracleNet:

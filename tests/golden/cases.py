@@ -36,15 +36,24 @@ CASES = {
 # the reference refuses networks of 6x6 modules and more; the 2x2 network
 # is the benchmark one, which the reference accepts as it is.  Per case: the network, the
 # ranks whose BACKWARD synapse dump is hashed, and the window (ms) of the
-# per-population firing statistics.
+# per-population firing statistics.  (The reference writes the dump of rank
+# 0 only, DPSNN_localNet_init.c:786.)
 SUMMARY_CASES = {
     # the benchmark network, 192 ranks (3 modules each), over its onset burst
     "c2_24x24_p192": (lambda: nc.cortical_grid(24, 24, total_ms=100, glob_h=192, delay_range_subpop=True),
-                      (0, 1, 95, 191), (20, 100)),
+                      (0,), (20, 100)),
     # 6x6 modules, 12 ranks, 10 s: the bit-identical window and, after it,
     # the firing statistics
     "c_6x6_p12_10s": (lambda: nc.cortical_grid(6, 6, total_ms=10000, glob_h=12, delay_range_subpop=True),
-                      (0, 11), (1000, 10000)),
+                      (0,), (1000, 10000)),
     # the 2x2 benchmark network, 1 rank, 10 s
     "c1_2x2_10s": (lambda: nc.cortical_grid(2, 2, total_ms=10000), (0,), (1000, 10000)),
+}
+
+
+# Networks the reference refuses to build; make_golden.py records its error
+# line.  6x6 modules with delays 1-20 ms: one of the ~50 M delay draws
+# reaches the float level 80 of getRandomDelay_UNI.
+REFUSED_CASES = {
+    "refused_6x6_p12": lambda: nc.cortical_grid(6, 6, total_ms=10, glob_h=12),
 }

@@ -23,11 +23,17 @@ built from the unmodified sources plus the bounds fix:
 * ``<case>.summary.npz`` for the networks of ``SUMMARY_CASES``, whose
                           raster is too large to commit: per emission ms the
                           spike count and CRC-32, per rank the raster's
-                          SHA-256 (see tests/golden/io.py); their manifest
+                          SHA-256 (see tests/golden/io.py), and per step the
+                          synaptic events that raster delivers (with the
+                          restatement's out-degree per neuron and delay);
+                          their manifest
                           entry holds the BACKWARD dump SHA-256 of a few
                           ranks and the per-population firing rates and ISI
                           CV.  Those runs write the other ranks' synapse
                           dumps to /dev/null.
+
+* the manifest entry of each network of ``REFUSED_CASES`` holds the first
+  ERROR line the reference printed when it refused to build it.
 
 Usage: python tests/golden/make_golden.py [case ...]
 (with case names, only those entries of the manifest are regenerated)
@@ -48,7 +54,7 @@ import tempfile
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
-from tests.golden.cases import CASES, SUMMARY_CASES  # noqa: E402
+from tests.golden.cases import CASES, REFUSED_CASES, SUMMARY_CASES  # noqa: E402
 from tests.golden import io as gio  # noqa: E402
 
 nc = importlib.import_module("201812realtimecortsim_b200.netconfig")
@@ -129,12 +135,33 @@ def make_summary(name, manifest):
         ids, ts = read_raster(hp, cfg)
     cnt, crc = gio.per_ms_digests(ids, ts, cfg.total_ms)
     rd = gio.rank_digests(ids, ts, cfg.glob_h, cfg.glob_n)
+    # synaptic events per step (addInputSpike calls, which the reference
+    # does not print): the reference's raster over the out-degree per
+    # (neuron, delay) of the restatement's generation
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import dpsnn_oracle as O
+    ev = O.events_per_step(O.outdegree_by_delay(cfg), ids, ts, cfg.total_ms)
     np.savez_compressed(os.path.join(HERE, f"{name}.summary.npz"), count_per_ms=cnt, crc_per_ms=crc,
-                        rank_sha256=rd)
+                        rank_sha256=rd, events_per_step=ev)
     rates, cvs = gio.pop_stats(ids, ts, [p.count for p in cfg.subpops], cfg.glob_n, w0, w1)
     entry.update({"spikes": int(len(ids)), "stats_window_ms": [w0, w1], "rates_hz": rates, "isi_cv": cvs})
     manifest[name] = entry
     print(name, len(ids), "spikes", rates, cvs, flush=True)
+
+
+def make_refused(name, manifest):
+    """Run a network the reference refuses; record its first ERROR line."""
+    cfg = REFUSED_CASES[name]()
+    with tempfile.TemporaryDirectory() as td:
+        env = dict(os.environ)
+        env.update(cfg.write(td))
+        env["DPSNN_SHM_RANKS"] = str(cfg.glob_h)
+        r = subprocess.run([REF_MP if cfg.glob_h > 1 else REF], cwd=td, env=env, capture_output=True, text=True)
+    errors = [l for l in r.stdout.splitlines() if l.startswith("ERROR")]
+    if not errors:
+        raise RuntimeError(f"{name}: the reference did not refuse the network")
+    manifest[name] = {"refused": errors[0], "glob_h": cfg.glob_h}
+    print(name, errors[0], flush=True)
 
 
 def main():
@@ -150,6 +177,9 @@ def main():
     for name in SUMMARY_CASES:
         if only and name in only:
             make_summary(name, manifest)
+    for name in REFUSED_CASES:
+        if not only or name in only:
+            make_refused(name, manifest)
     for name, make in CASES.items():
         if only and name not in only:
             continue

@@ -29,8 +29,25 @@ def test_localnet_exports_the_dal_trio_with_cxx_linkage():
     main leaves undefined (C++ names of localNetProcess.h:72-74)."""
     lib = C.CDLL(os.path.join(ROOT, "201812realtimecortsim_b200", "libdpsnn_localnet.so"))
     for sym in ("_Z20localNetProcess_initP8_process", "_Z20localNetProcess_fireP8_process",
-                "_Z22localNetProcess_finishP8_process"):
+                "_Z22localNetProcess_finishP8_process", "_Z13getParametersj"):
         assert hasattr(lib, sym), sym
+
+
+def test_localnet_getparameters_reads_the_run_inputs(tmp_path, monkeypatch):
+    """getParameters(loc_h) (C++ name of DPSNN_getParameters.h:7) parses the
+    env_* variables and the input files of the current directory."""
+    cfg = CASES["small_2x2"]()
+    _env_for(cfg, tmp_path, monkeypatch)
+    monkeypatch.chdir(tmp_path)
+    lib = C.CDLL(os.path.join(ROOT, "201812realtimecortsim_b200", "libdpsnn_localnet.so"))
+    f = lib._Z13getParametersj
+    f.restype = E.Params
+    f.argtypes = [C.c_uint32]
+    got = f(0)
+    want = E.params_from_env(str(tmp_path)).p
+    for field in ("cfx", "cfy", "glob_h", "D", "nsub", "global_seed", "stencil_dim"):
+        assert getattr(got, field) == getattr(want, field), field
+    assert list(got.count) == list(want.count)
 
 
 def test_binding_covers_the_header():

@@ -6,7 +6,7 @@ import pytest
 import dpsnn_oracle as O
 from tests.conftest import engine_module, netconfig
 from tests.golden import io as gio
-from tests.golden.cases import CASES, small
+from tests.golden.cases import CASES, REFUSED_CASES, small
 
 pytestmark = pytest.mark.gpu
 E = engine_module()
@@ -89,7 +89,7 @@ def test_stdp_weights_and_traces_match_oracle():
 
 def test_run_to_run_determinism_large_grid():
     # 6x6 grid, 12 emulated ranks: atomics in delivery must not change results.
-    cfg = nc.cortical_grid(6, 6, total_ms=60, glob_h=12)
+    cfg = nc.cortical_grid(6, 6, total_ms=60, glob_h=12, delay_range_subpop=True)
     a, ia, ta = run_engine(cfg, 60)
     b, ib, tb = run_engine(cfg, 60)
     np.testing.assert_array_equal(ia, ib)
@@ -102,7 +102,7 @@ def test_run_to_run_determinism_large_grid():
 def test_full_size_grid_invariants():
     # 24x24 grid (720000 neurons, ~0.81 G synapses), 192 emulated ranks:
     # size-independent properties of the connectome and of the dynamics.
-    cfg = nc.cortical_grid(24, 24, total_ms=40, glob_h=192)
+    cfg = nc.cortical_grid(24, 24, total_ms=40, glob_h=192, delay_range_subpop=True)
     eng = E.Engine(cfg)
     S = eng.synapse_count
     assert 0.79e9 < S < 0.83e9                   # mean in-degree ~1125
@@ -115,3 +115,14 @@ def test_full_size_grid_invariants():
         if len(te):
             assert te.min() >= t - 1 and te.max() < t             # emitted in step t-1
     assert eng.events_delivered() > 0
+
+
+@pytest.mark.parametrize("name", sorted(REFUSED_CASES))
+def test_refuses_what_the_reference_refuses(name):
+    # e.g. 6x6 modules with delays 1-20 ms (no delay-range sub-population):
+    # one of the ~50 M delay draws reaches level 80, where getRandomDelay_UNI
+    # (DPSNN_LIFCAcorticalModuleGen.cpp:322-326) stops the reference with
+    # "delay level generated ... max allowed delay levels"
+    assert "delay level generated" in gio.manifest()[name]["refused"]
+    with pytest.raises(E.EngineError, match="delay level generated"):
+        E.Engine(REFUSED_CASES[name]())

@@ -12,7 +12,7 @@ import pytest
 
 import dpsnn_oracle as O
 from tests.golden import io as gio
-from tests.golden.cases import CASES
+from tests.golden.cases import CASES, REFUSED_CASES
 
 MANIFEST = gio.manifest()
 
@@ -92,3 +92,23 @@ def test_correctly_rounded_libm_matches_system_on_2x2():
     sa, sb = a.state(), b.state()
     for k in sa:
         np.testing.assert_array_equal(sa[k], sb[k])
+
+
+@pytest.mark.parametrize("name", sorted(REFUSED_CASES))
+def test_restatement_refuses_what_the_reference_refuses(name):
+    """The reference stopped building this network (its error line is in the
+    manifest); the restatement's generation stops too."""
+    assert "delay level generated" in MANIFEST[name]["refused"]
+    with pytest.raises(RuntimeError, match="delay level generated"):
+        O.outdegree_by_delay(REFUSED_CASES[name]())
+
+
+@pytest.mark.parametrize("name", ["c1_2x2", "small_2x2_p4"])
+def test_events_from_raster_and_outdegree(name):
+    """Events per step counted from the reference's raster over the
+    restatement's out-degree per (neuron, delay) equal the events the
+    restatement delivers when it runs (the count the summaries use)."""
+    cfg = CASES[name]()
+    gi, gt = gio.raster(name)
+    ev = O.events_per_step(O.outdegree_by_delay(cfg), gi.astype(np.int64), gt, cfg.total_ms)
+    assert int(ev.sum()) == MANIFEST[name]["events"]
