@@ -283,6 +283,18 @@ __device__ static inline uint32_t random_delay_exp(const NetConst *net, Ran3 &g,
   return outfunc;
 }
 
+#define GEN_THREADS 16          // generation streams per block
+#define GEN_TL_SMEM 2048        // targets of a neuron held in shared memory
+#define GEN_TL_STRIDE (GEN_TL_SMEM + 1)   // odd stride: threads' lists in different banks
+#define GEN_SMEM ((size_t)GEN_THREADS * (sizeof(Ran3) + 4 * GEN_TL_STRIDE + 2 * RING_SLOTS))
+
+// A neuron's target list: the first GEN_TL_SMEM entries in shared memory,
+// the rest (rare: in-degrees are ~1100) in the thread's global scratch.
+struct GenTargets {
+  uint32_t *sh, *gl;
+  __device__ uint32_t &operator[](uint32_t j) const { return j < GEN_TL_SMEM ? sh[j] : gl[j]; }
+};
+
 __global__ void gen_kernel(const NetConst *__restrict__ net, const float *__restrict__ prob, int pass,
                            GenRecord *rec, const int32_t *__restrict__ chosen_hyp,
                            const double *__restrict__ chosen_cache, uint16_t *cnt_out,
@@ -290,6 +302,14 @@ __global__ void gen_kernel(const NetConst *__restrict__ net, const float *__rest
                            uint32_t *post, int16_t *w16, uint32_t *scratch,
                            const uint32_t *__restrict__ bath_tmpl, double *inv_nu,
                            uint32_t *max_ext, uint8_t *sub) {
+  // Each thread's serial stream keeps its ran3 table, the current neuron's
+  // target list (its first GEN_TL_SMEM entries; more go to the global
+  // scratch) and the per-delay counts in shared memory: the stream is a long
+  // chain of dependent table reads.
+  extern __shared__ __align__(16) unsigned char gen_smem_raw[];
+  Ran3 *s_rng = reinterpret_cast<Ran3 *>(gen_smem_raw);
+  uint32_t *s_tl = reinterpret_cast<uint32_t *>(s_rng + blockDim.x);
+  uint16_t *s_cnt = reinterpret_cast<uint16_t *>(s_tl + (size_t)blockDim.x * GEN_TL_STRIDE);
   uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t nthreads = (pass == 0) ? 2 * net->nmod : net->nmod;
   if (tid >= nthreads) return;
@@ -297,10 +317,10 @@ __global__ void gen_kernel(const NetConst *__restrict__ net, const float *__rest
   int hyp = (pass == 0) ? (int)(tid & 1) : chosen_hyp[m];
   GenRecord *R = &rec[(pass == 0) ? tid : m];
   const uint32_t N = net->N, D = net->D, npcm = net->npcm, stencil = net->stencil;
-  uint32_t *tl = scratch + (size_t)tid * MAX_SYN_PER_NEURON;
-  uint16_t cnt[RING_SLOTS];
+  GenTargets tl{s_tl + (size_t)threadIdx.x * GEN_TL_STRIDE, scratch + (size_t)tid * MAX_SYN_PER_NEURON};
+  uint16_t *cnt = s_cnt + (size_t)threadIdx.x * RING_SLOTS;
 
-  Ran3 g;
+  Ran3 &g = s_rng[threadIdx.x];
   g.iff = 0;
   g.idum = 0;
   g.inext = g.inextp = 0;
@@ -451,6 +471,7 @@ struct Dev {
   const uint32_t *fix_bitmap; // one bit per float in [0x30000000, 0x3F800000]: key has a fix-up
   // control
   uint32_t *t;              // current step
+  uint32_t *bath_t;         // step of the next bath launch (the bath runs one step ahead)
   uint32_t *flags;
   unsigned long long *events;  // synaptic events delivered
 };
@@ -687,36 +708,55 @@ __global__ void __launch_bounds__(DELIVER_THREADS) deliver_kernel(Dev d) {
 //              lapse factor -logf((float)(1-u)), and extend q[], the running
 //              sum over draws of one parity of the lapses in 2^-20 units
 //              (q[n] = q[n-2] + round(lap[n] * 2^20), integers mod 2^32);
-//   warp 4     stays idle: warps go to the SM's four schedulers by index, so
+//   warps 4, 8 stay idle: warps go to the SM's four schedulers by index, so
 //              this leaves warp 0 a scheduler of its own;
-//   warp 0     walks the neurons.  The number of events c of a neuron is the
-//              first c at which nextBath + sum of c lapses * invNuExt reaches
-//              t+1.  Per chunk of 32 neurons each lane turns its neuron's
-//              budget (t+1 - nextBath)/invNuExt into two integer bounds that
-//              enclose every rounding of the reference's sequential sum; on
-//              the serial chain, lane L compares the sum of the next L+1
-//              lapses (two q[] reads) with the bounds and one ballot gives c.
-//              Where a sum falls between the bounds (or c > 32, or the
-//              maxExternCurrentCount cap is reached), the reference's
-//              sequential loop decides instead.
-//              Then the 32 lanes write a 32-neuron chunk's events in
-//              parallel, each replaying its neuron in the reference's exact
-//              arithmetic.
+//   warps 5-7, 9-11 tabulate the event counts of the next chunk of 32
+//              neurons.  The number of events c of a neuron is the first c
+//              at which nextBath + sum of c lapses * invNuExt reaches t+1; it
+//              depends on where in the stream the neuron starts, which is
+//              known only once every earlier neuron of the rank is decided.
+//              Each lane turns its neuron's budget (t+1 - nextBath)/invNuExt
+//              into two integer bounds that enclose every rounding of the
+//              reference's sequential sum, predicts the neuron's start from
+//              the chunk's published start and the expected counts
+//              (1 + budget each), and for the BATH_NC candidate starts around
+//              it finds c by a binary search of q[] (c - 1 sums below the
+//              lower bound, the c-th at or above the upper one); a candidate
+//              the bounds do not decide is marked undecided;
+//   warp 0     walks the neurons: per neuron one table lookup at its actual
+//              start gives c, so the serial chain is a subtraction, a shared
+//              load and an addition.  An undecided entry, a start outside
+//              the window, or the maxExternCurrentCount cap falls back to the
+//              reference's sequential loop.
+//              Then the 32 lanes write a chunk's events in parallel, each
+//              replaying its neuron in the reference's exact arithmetic.
 // Rounds are published in order with a flag; every wait is bounded and
 // raises F_BATH_DRAWS when its limit is reached.
-#define BATH_THREADS 256
+#define BATH_THREADS 384       // 12 warps: roles in bath_kernel
 #define BATH_RING 8192         // draws resident in shared memory
 #define BATH_ROUNDS 512        // round flags tracked (BATH_ROUNDS*24 > BATH_RING)
 #define BATH_MAX_EXT 2048      // largest maxExternCurrentCount supported
 #define BATH_SPIN_LIMIT (1u << 26)
-#define BATH_FAST_LANES 32     // events decided by one ballot
-#define BATH_IDLE_WARP 4       // shares the consumer's scheduler: left idle
-#define BATH_WINDOW (2 * BATH_FAST_LANES + 2)   // draws a ballot reads past pos
+#define BATH_FAST_LANES 32     // events decided by one count table entry
+#define BATH_WINDOW (2 * BATH_FAST_LANES + 2)   // draws a count decision reads past its start
+#define BATH_NC 64             // candidate start positions tabulated per neuron
+#define BATH_BUILDERS 6        // table-building warps: 5, 6, 7, 9, 10, 11
+#define BATH_AHEAD 2           // chunks the count tables are built ahead of the consumer (the code below
+                               // predicts from chunk c-2's start)
+#define BATH_TABS (BATH_AHEAD + 1)
 
 struct BathSmem {
   uint32_t lap[BATH_RING];          // raw draw until converted, then the lapse (float bits)
   uint32_t q[BATH_RING];            // per-parity prefix of the lapses, 2^-20 units
   uint8_t idx[BATH_RING];
+  uint8_t tab[BATH_TABS][BATH_NC + 1][32];  // chunk c % BATH_TABS: events of neuron L started at
+                                    // bp_base + 2o, 0xFF = undecided; row BATH_NC: 0xFF (outside the window)
+  uint32_t bp_base[BATH_TABS][32];  // position (low 32 bits) of candidate 0 of neuron L
+  uint32_t bp_misc[BATH_TABS][32];  // 0: no bath event this step
+  uint32_t tab_cnt[BATH_TABS];      // builder-warp completions of the tables of this buffer
+  uint32_t c_start[32], c_cnt[32];  // the consumer's decisions for the chunk being emitted
+  unsigned long long chunk_start[BATH_TABS];  // exact start of chunk c (consumer, as it begins chunk c)
+  uint32_t chunk_seq;               // chunks whose start is published
   uint32_t flag[BATH_ROUNDS];       // round r converted <=> flag[r % BATH_ROUNDS] == r + 1
   uint32_t hist[64];
   unsigned long long pos;           // consumer position (draws)
@@ -759,7 +799,84 @@ __device__ static inline uint32_t lap_fixed(float lap) {
   return __double2uint_rn((double)lap * 0x1p20);   // lap < 2^11: no overflow
 }
 
-__global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d, uint32_t t) {
+// Integer bounds on the lapse sum, in 2^-20 units, for one neuron: a
+// fixed-point sum F of c lapses below lo means the reference's sequential
+// nextBath after c events is certainly < t+1, at or above hi1 certainly
+// >= t+1.  E1 bounds the rounding of that sequential sum (c <= 32
+// additions, |values| < |T1| + 42 invNuExt, and t+1 - nextBath); 2^-16
+// bounds the rounding of F (32 terms of at most 2^-21); the 2^-30 relative
+// margin covers the bound's own arithmetic.  Both are clamped to 32 bits
+// (F < 2^30).  misc: 0 = no bath event this step; else 0x100 |
+// min(32, maxExternCurrentCount).
+__device__ static inline void bath_bounds(double T1, double nb, double inv, uint32_t mx, uint32_t &lo,
+                                          uint32_t &hi1, uint32_t &misc) {
+  lo = hi1 = misc = 0;
+  if (inv > 0 && nb < T1) {
+    const double E1 = 0x1p-44 * (fabs(T1) + fabs(nb) + 1.0 + 32.0 * inv);
+    double blo = ((T1 - nb) - E1) / inv - 0x1p-16;
+    double bhi = ((T1 - nb) + E1) / inv + 0x1p-16;
+    const double mg = 0x1p-30 * (fabs(bhi) + 1.0);
+    blo = fmin(fmax(floor((blo - mg) * 0x1p20), 0.0), 4294967295.0);
+    bhi = fmin(fmax(ceil((bhi + mg) * 0x1p20) + 1.0, 0.0), 4294967295.0);
+    lo = (uint32_t)blo;
+    hi1 = (uint32_t)bhi;
+    misc = 0x100u | min(32u, mx);
+  }
+}
+
+// The reference's loop for one neuron from stream position pos
+// (regularDynamicTimeStep, DPSNN_neuron_sim.c:604-640): the events go to c,
+// the position after the neuron's draws is returned.  Waits (bounded) until
+// the draws it reads are converted; sets fail when a wait gives up.
+__device__ static inline unsigned long long bath_exact(BathSmem &s, double nbv, double inv, uint32_t mx, double T1,
+                                                       unsigned long long pos, unsigned long long &lim, uint32_t &rr,
+                                                       uint32_t &spins, bool &fail, uint32_t &c) {
+  volatile BathSmem &vs = s;
+  const uint32_t M = BATH_RING - 1;
+  c = 0;
+  while (lim < pos + 2ull * mx + 4) {
+    if (vs.flag[rr % BATH_ROUNDS] == rr + 1) {
+      rr++;
+      lim = s.conv_base + (unsigned long long)rr * 24;
+      __threadfence_block();
+    } else if (++spins > BATH_SPIN_LIMIT) {
+      fail = true;
+      return pos;
+    }
+  }
+  float ln = __uint_as_float(s.lap[(pos + 1) & M]);
+  do {
+    c++;
+    const double step = (double)ln * inv;
+    pos += 2;
+    ln = __uint_as_float(s.lap[(pos + 1) & M]);
+    nbv += step;
+  } while ((nbv < T1) && (c < mx));
+  if (c >= mx && nbv < T1) {
+    do {   // single draws past the cap (rare)
+      while (lim <= pos) {
+        if (vs.flag[rr % BATH_ROUNDS] == rr + 1) {
+          rr++;
+          lim = s.conv_base + (unsigned long long)rr * 24;
+          __threadfence_block();
+        } else if (++spins > BATH_SPIN_LIMIT) {
+          fail = true;
+          return pos;
+        }
+      }
+      nbv += (double)__uint_as_float(s.lap[pos & M]) * inv;
+      pos += 1;
+    } while (nbv < T1);
+  }
+  return pos;
+}
+
+__device__ static inline int bath_builder_index(uint32_t warp) {
+  return (warp >= 5 && warp <= 7) ? (int)warp - 5 : (warp >= 9 && warp <= 11) ? (int)warp - 6 : -1;
+}
+
+__global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
+  const uint32_t t = *d.bath_t;
   extern __shared__ __align__(16) unsigned char bath_smem_raw[];
   BathSmem &s = *reinterpret_cast<BathSmem *>(bath_smem_raw);
   volatile BathSmem &vs = s;
@@ -783,6 +900,11 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d, uint32_t t) {
     s.published = 0;
     s.done = 0;
     s.err = 0;
+    s.chunk_seq = 0;
+    for (int b = 0; b < BATH_TABS; b++) {
+      s.tab_cnt[b] = 0;
+      for (int l = 0; l < 32; l++) s.tab[b][BATH_NC][l] = 0xFF;
+    }
     s.q[(p0 - 2) & M] = 0;   // the prefix starts at p0 in each launch
     s.q[(p0 - 1) & M] = 0;
   }
@@ -833,7 +955,140 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d, uint32_t t) {
       if (lane == 0) vs.raw_end = n0 + 24;
       r++;
     }
-  } else if (warp >= 2 && warp != BATH_IDLE_WARP) {
+  } else if (bath_builder_index(warp) >= 0) {
+    // ---- count tables, one chunk ahead of the consumer
+    const uint32_t bw = (uint32_t)bath_builder_index(warp);
+    unsigned long long pred = p0;   // predicted start of chunk c
+    uint32_t exp1 = 0, exp2 = 0;    // expected events of chunks c-1 and c-2
+    unsigned long long lim = s.raw_end;
+    uint32_t rr = 0, spins = 0;
+    bool fail = false;
+    // What does not depend on where a chunk starts -- each lane's neuron,
+    // its bounds and expected events, their prefix over the chunk -- is
+    // prepared a chunk early: the next chunk's loads are in flight while
+    // this chunk's candidates are evaluated.
+    uint32_t n_lo = 0, n_hi1 = 0, n_misc = 0, n_ec = 0, n_incl = 0;
+    double x_nb = 0, x_inv = 0;
+    uint32_t x_mx = 0;
+    auto prepare = [&](uint32_t cc0) {
+      const uint32_t ccn = min(32u, locN - cc0);
+      n_lo = n_hi1 = n_misc = n_ec = 0;
+      if (lane < ccn) {
+        bath_bounds(T1, x_nb, x_inv, x_mx, n_lo, n_hi1, n_misc);
+        if (n_misc) n_ec = 1u + (uint32_t)fmin(rint((T1 - x_nb) / x_inv), 64.0);   // expected events: 1 + budget
+      }
+      n_incl = n_ec;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, n_incl, o);
+        if (lane >= (uint32_t)o) n_incl += y;
+      }
+    };
+    if (lane < min(32u, locN)) {
+      x_nb = d.nb_prev[i0 + lane];
+      x_inv = d.inv_nu[i0 + lane];
+      x_mx = d.max_ext[i0 + lane];
+    }
+    prepare(0);
+    for (uint32_t c = 0, c0 = 0; c0 < locN; c++, c0 += 32) {
+      const uint32_t cn = min(32u, locN - c0), b = c % BATH_TABS;
+      const uint32_t lo = n_lo, hi1 = n_hi1, misc = n_misc, ec = n_ec, incl = n_incl;
+      if (c0 + 32 < locN && lane < min(32u, locN - c0 - 32)) {   // the next chunk's neurons
+        x_nb = d.nb_prev[i0 + c0 + 32 + lane];
+        x_inv = d.inv_nu[i0 + c0 + 32 + lane];
+        x_mx = d.max_ext[i0 + c0 + 32 + lane];
+      }
+      // the prediction starts from the latest chunk start known for sure,
+      // chunk c-2's (BATH_AHEAD = 2), published by the consumer as it begins
+      // that chunk (so it is also done with this buffer's previous tables),
+      // plus the expected events of chunks c-2 and c-1; chunk 0 starts at p0
+      unsigned long long floor_pos = p0;
+      if (c >= 3) {
+        while (vs.chunk_seq < c - 1) {
+          if (vs.done) { fail = true; break; }
+          if (++spins > BATH_SPIN_LIMIT) { vs.err = 1; vs.done = 1; fail = true; break; }
+          __nanosleep(32);
+        }
+        if (fail) break;
+        __threadfence_block();
+        floor_pos = vs.chunk_start[(c - 2) % BATH_TABS];
+      }
+      pred = floor_pos + 2ull * ((c >= 2 ? exp2 : 0u) + (c >= 1 ? exp1 : 0u));
+      exp2 = exp1;
+      exp1 = __shfl_sync(0xffffffffu, incl, 31);
+      // candidate o of this lane's neuron starts at base + 2o, the
+      // prediction in the middle of the window
+      const unsigned long long base = pred + 2ull * (incl - ec) - BATH_NC;
+      if (bw == 0) {
+        s.bp_base[b][lane] = (uint32_t)base;
+        s.bp_misc[b][lane] = misc;
+      }
+      // the draws every candidate of the chunk reads are converted; never
+      // beyond what the generator may produce ahead of the consumer (at
+      // least floor_pos + BATH_RING - 64): candidates past that stay undecided
+      const unsigned long long reach = floor_pos + BATH_RING - 512;
+      const unsigned long long need =
+          min(__shfl_sync(0xffffffffu, base, 31) + 2ull * BATH_NC + BATH_WINDOW, reach);
+      while (lim < need) {
+        if (vs.flag[rr % BATH_ROUNDS] == rr + 1) {
+          rr++;
+          lim = s.conv_base + (unsigned long long)rr * 24;
+          __threadfence_block();
+        } else if (vs.done) {
+          fail = true;
+          break;
+        } else if (++spins > BATH_SPIN_LIMIT) {
+          vs.err = 1;
+          vs.done = 1;
+          fail = true;
+          break;
+        } else {
+          __nanosleep(32);
+        }
+      }
+      if (fail) break;
+      if (lane < cn && misc) {
+        // this warp's candidates o = bw, bw + BATH_BUILDERS, ..; for a start
+        // P the count is m + 1, m the number of k < 32 whose sum of the
+        // k+1 lapses at P+1, P+3, .., P+1+2k is below lo (the sums grow with
+        // k), when the (m+1)-th sum reaches hi1.  Positions are taken modulo
+        // 2^32 (a step reads far fewer draws); four candidates' binary
+        // searches run in lockstep, each probe round four independent loads.
+        const uint32_t cap = misc & 0xFFu, b32 = (uint32_t)base, f32 = (uint32_t)floor_pos;
+        const uint32_t r32 = (uint32_t)reach - BATH_WINDOW;
+        for (uint32_t o0 = bw; o0 < BATH_NC; o0 += 4 * BATH_BUILDERS) {
+          uint32_t P[4], qb[4], m[4];
+          bool ok[4];
+#pragma unroll
+          for (int v = 0; v < 4; v++) {
+            const uint32_t o = o0 + v * BATH_BUILDERS;
+            P[v] = b32 + 2u * o;
+            ok[v] = o < BATH_NC && (int32_t)(P[v] - f32) >= 0 && (int32_t)(r32 - P[v]) >= 0;
+            qb[v] = s.q[(P[v] - 1) & M];
+            m[v] = 0;
+          }
+#pragma unroll
+          for (uint32_t st = 16; st > 0; st >>= 1) {
+            uint32_t f[4];
+#pragma unroll
+            for (int v = 0; v < 4; v++) f[v] = s.q[(P[v] + 1 + 2 * (m[v] + st - 1)) & M];
+#pragma unroll
+            for (int v = 0; v < 4; v++) m[v] += (f[v] - qb[v] < lo) ? st : 0u;
+          }
+#pragma unroll
+          for (int v = 0; v < 4; v++) {
+            const uint32_t F = s.q[(P[v] + 1 + 2 * m[v]) & M] - qb[v];
+            const uint32_t mm = (m[v] == 31 && F < lo) ? 32u : m[v];
+            const uint32_t o = o0 + v * BATH_BUILDERS;
+            if (o < BATH_NC) s.tab[b][o][lane] = (ok[v] && mm < cap && F >= hi1) ? (uint8_t)(mm + 1) : (uint8_t)0xFF;
+          }
+        }
+      }
+      __syncwarp();
+      __threadfence_block();
+      if (lane == 0) atomicAdd(&s.tab_cnt[b], 1u);
+      if (c0 + 32 < locN) prepare(c0 + 32);
+    }
+  } else if (warp == 2 || warp == 3) {
     // ---- converters: rounds are claimed in order and published in order
     while (true) {
       uint32_t r = 0;
@@ -898,46 +1153,33 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d, uint32_t t) {
       nx_inv = d.inv_nu[i0 + lane];
       nx_mx = d.max_ext[i0 + lane];
     }
-    for (uint32_t c0 = 0; c0 < locN && !fail; c0 += 32) {
-      const uint32_t cn = min(32u, locN - c0);
+    for (uint32_t c0 = 0, ck = 0; c0 < locN && !fail; c0 += 32, ck++) {
+      const uint32_t cn = min(32u, locN - c0), tb = ck % BATH_TABS;
       const double my_nb = nx_nb, my_inv = nx_inv;
       const uint32_t my_mx = nx_mx;
-      // Integer bounds on the lapse sum, in 2^-20 units, for this lane's
-      // neuron: a fixed-point sum F of c lapses below my_lo means the
-      // reference's sequential nextBath after c events is certainly < t+1,
-      // above my_hi certainly >= t+1.  E1 bounds the rounding of that
-      // sequential sum (c <= 32 additions, |values| < |T1| + 42 invNuExt,
-      // and t+1 - nextBath); 2^-16 bounds the rounding of F (32 terms of at
-      // most 2^-21); the 2^-30 relative margin covers the bound's own
-      // arithmetic.
-      // my_lo / my_hi1: F < my_lo means certainly below, F >= my_hi1
-      // certainly reached, both clamped to 32 bits (F < 2^30).  my_misc:
-      // 0 = no bath event this step; else 0x100 | min(32, maxExternCurrentCount).
-      uint32_t my_lo = 0, my_hi1 = 0, my_misc = 0;
-      if (my_inv > 0 && my_nb < T1) {
-        const double E1 = 0x1p-44 * (fabs(T1) + fabs(my_nb) + 1.0 + 32.0 * my_inv);
-        double blo = ((T1 - my_nb) - E1) / my_inv - 0x1p-16;
-        double bhi = ((T1 - my_nb) + E1) / my_inv + 0x1p-16;
-        const double mg = 0x1p-30 * (fabs(bhi) + 1.0);
-        blo = fmin(fmax(floor((blo - mg) * 0x1p20), 0.0), 4294967295.0);
-        bhi = fmin(fmax(ceil((bhi + mg) * 0x1p20) + 1.0, 0.0), 4294967295.0);
-        my_lo = (uint32_t)blo;
-        my_hi1 = (uint32_t)bhi;
-        my_misc = 0x100u | min(32u, my_mx);
+      // this chunk's count table, then its start for the builders
+      {
+        uint32_t sp = 0;
+        while (vs.tab_cnt[tb] < BATH_BUILDERS * (ck / BATH_TABS + 1)) {
+          if (vs.done || ++sp > BATH_SPIN_LIMIT) { fail = true; break; }
+          __nanosleep(20);   // leave the shared-memory pipe to the builders
+        }
+        if (fail) break;
+        __threadfence_block();
+        if (lane == 0) {
+          vs.chunk_start[ck % BATH_TABS] = pos;
+          __threadfence_block();
+          vs.chunk_seq = ck + 1;
+        }
       }
       if (c0 + 32 < locN && lane < min(32u, locN - c0 - 32)) {   // prefetch the next chunk
         nx_nb = d.nb_prev[i0 + c0 + 32 + lane];
         nx_inv = d.inv_nu[i0 + c0 + 32 + lane];
         nx_mx = d.max_ext[i0 + c0 + 32 + lane];
       }
-      unsigned long long my_start = 0;
-      uint32_t my_cnt = 0;
-      // One wait covers the whole chunk while every neuron takes the fast
-      // path (at most 2 * BATH_FAST_LANES draws each); after a fall-back the
-      // bound is checked per neuron again.
+      // the chunk's draws are converted (at most 2 * BATH_FAST_LANES per
+      // neuron through the table; a fall-back waits again for itself)
       const unsigned long long base = pos;
-      uint32_t rel = 0;   // pos - base
-      bool safe = true;
       uint32_t spins = 0;
       while (lim < base + 64ull * BATH_FAST_LANES + BATH_WINDOW) {
         if (vs.flag[rr % BATH_ROUNDS] == rr + 1) {
@@ -950,90 +1192,47 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d, uint32_t t) {
         }
       }
       if (fail) break;
-#pragma unroll 2
-      for (uint32_t j = 0; j < cn; j++) {
-        const uint32_t lo = __shfl_sync(0xffffffffu, my_lo, j);
-        const uint32_t hi1 = __shfl_sync(0xffffffffu, my_hi1, j);
-        const uint32_t misc = __shfl_sync(0xffffffffu, my_misc, j);
-        if (!safe) {
-          while (lim < base + rel + BATH_WINDOW) {
-            if (vs.flag[rr % BATH_ROUNDS] == rr + 1) {
-              rr++;
-              lim = s.conv_base + (unsigned long long)rr * 24;
-              __threadfence_block();
-            } else if (++spins > BATH_SPIN_LIMIT) {
-              fail = true;
-              break;
-            }
+      // the serial chain: per neuron one table lookup at its actual start
+      const uint32_t *bb = s.bp_base[tb], *bm = s.bp_misc[tb];
+      const uint8_t *tab = &s.tab[tb][0][0];
+      uint32_t P = (uint32_t)base;
+      for (uint32_t j0 = 0; j0 < 32;) {
+        // a run with no branch on the chain: out-of-window starts read the
+        // sentinel row; the first undecided neuron is redone below
+        uint32_t bad = 32;
+#pragma unroll 4
+        for (uint32_t j = j0; j < 32; j++) {
+          const uint32_t dl = P - bb[j];
+          const uint32_t row = ((dl & ~(uint32_t)(2 * BATH_NC - 2)) == 0) ? (dl >> 1) : (uint32_t)BATH_NC;
+          uint32_t cv = tab[row * 32 + j];
+          cv = bm[j] ? cv : 0u;
+          bad = (bad == 32 && cv == 0xFFu) ? j : bad;
+          if (lane == 0) {
+            s.c_start[j] = P;
+            s.c_cnt[j] = cv;
           }
-          if (fail) break;
+          P += 2 * (cv & 0x3Fu);
         }
-        const uint32_t start_rel = rel;
-        uint32_t c = 0;
-        if (misc) {
-          // lane L: the lapses at pos+1, pos+3, .., pos+1+2L, in 2^-20 units
-          const uint32_t p32 = (uint32_t)base + rel;
-          const uint32_t F = s.q[(p32 + 1 + 2 * lane) & M] - s.q[(p32 - 1) & M];
-          const uint32_t below = __ballot_sync(0xffffffffu, F < lo);
-          const uint32_t above = __ballot_sync(0xffffffffu, F >= hi1);
-          const uint32_t m = __popc(below);   // F grows with L: below is a prefix
-          if (m < (misc & 0xFFu) && ((above >> m) & 1u)) {
-            c = m + 1;
-            rel += 2 * c;
-          } else {
-            safe = false;
-            pos = base + rel;
-            // the reference's loop (regularDynamicTimeStep :604-640)
-            double nbv = __shfl_sync(0xffffffffu, my_nb, j);
-            const double inv = __shfl_sync(0xffffffffu, my_inv, j);
-            const uint32_t mx = __shfl_sync(0xffffffffu, my_mx, j);
-            while (lim < pos + 2ull * mx + 4) {
-              if (vs.flag[rr % BATH_ROUNDS] == rr + 1) {
-                rr++;
-                lim = s.conv_base + (unsigned long long)rr * 24;
-                __threadfence_block();
-              } else if (++spins > BATH_SPIN_LIMIT) {
-                fail = true;
-                break;
-              }
-            }
-            if (fail) break;
-            float ln = __uint_as_float(s.lap[(pos + 1) & M]);
-            do {
-              c++;
-              const double step = (double)ln * inv;
-              pos += 2;
-              ln = __uint_as_float(s.lap[(pos + 1) & M]);
-              nbv += step;
-            } while ((nbv < T1) && (c < mx));
-            if (c >= mx && nbv < T1) {
-              do {   // single draws past the cap (rare)
-                while (lim <= pos) {
-                  if (vs.flag[rr % BATH_ROUNDS] == rr + 1) {
-                    rr++;
-                    lim = s.conv_base + (unsigned long long)rr * 24;
-                    __threadfence_block();
-                  } else if (++spins > BATH_SPIN_LIMIT) {
-                    fail = true;
-                    break;
-                  }
-                }
-                if (fail) break;
-                nbv += (double)__uint_as_float(s.lap[pos & M]) * inv;
-                pos += 1;
-              } while (nbv < T1);
-            }
-            rel = (uint32_t)(pos - base);
-          }
-        }
+        if (bad == 32) break;
+        // the reference's loop for neuron `bad` from its actual start, then
+        // the run goes on after it
+        __syncwarp();
+        P = s.c_start[bad];
+        const unsigned long long pj = base + (uint32_t)(P - (uint32_t)base);
+        uint32_t cx = 0;
+        const unsigned long long pe = bath_exact(s, __shfl_sync(0xffffffffu, my_nb, bad),
+                                                 __shfl_sync(0xffffffffu, my_inv, bad),
+                                                 __shfl_sync(0xffffffffu, my_mx, bad), T1, pj, lim, rr, spins, fail, cx);
         if (fail) break;
-        if (lane == j) {
-          my_start = base + start_rel;
-          my_cnt = c;
-        }
+        if (lane == 0) s.c_cnt[bad] = cx;
+        P = (uint32_t)pe;
+        j0 = bad + 1;
       }
-      pos = base + rel;
       if (fail) break;
+      __syncwarp();
+      const uint32_t my_cnt = (lane < cn) ? s.c_cnt[lane] : 0u;
+      const uint32_t my_start = s.c_start[lane];
+      pos = base + (uint32_t)(P - (uint32_t)base);
       // parallel emission of the chunk's events
       uint32_t incl = my_cnt;
       for (int o = 1; o < 32; o <<= 1) {
@@ -1332,52 +1531,78 @@ __device__ static inline uint32_t warp_path_max(const NetConst *net) {
 // lane's registers; the 15 farther ones (for E = 8) are one shuffle per
 // 32-bit word.  Ascending order at the end.
 template <int E>
+__device__ static inline void cas_in_lane(uint64_t (&tb)[E], uint32_t (&ky)[E], uint32_t (&wv)[E], int r, int q,
+                                          bool up) {
+  const bool gt = (tb[r] > tb[q]) || (tb[r] == tb[q] && ky[r] > ky[q]);
+  if (gt == up) {
+    const uint64_t t0 = tb[r];
+    tb[r] = tb[q];
+    tb[q] = t0;
+    const uint32_t k0 = ky[r];
+    ky[r] = ky[q];
+    ky[q] = k0;
+    const uint32_t w0 = wv[r];
+    wv[r] = wv[q];
+    wv[q] = w0;
+  }
+}
+
+// The in-lane stages j = J, J/2, .., 1 of one merge step k (k may be a
+// runtime value: the direction of a pair depends on bit k of its position).
+template <int E, int J>
+__device__ static inline void in_lane_stages(uint64_t (&tb)[E], uint32_t (&ky)[E], uint32_t (&wv)[E], uint32_t lane,
+                                             uint32_t k) {
+  if constexpr (J >= 1) {
+#pragma unroll
+    for (int r = 0; r < E; r++)
+      if (!(r & J)) cas_in_lane<E>(tb, ky, wv, r, r | J, ((lane * E + r) & k) == 0);
+    in_lane_stages<E, J / 2>(tb, ky, wv, lane, k);
+  }
+}
+
+// Bitonic sort of 32*E events held in registers, E per lane: element
+// e = lane*E + r sits in register r of its lane.  An element is (arrival
+// time as IEEE bits, key, weight): times are positive, so their bit
+// patterns order like the times, and equal times order by key, which is
+// unique per target.  Exchanges between positions closer than E stay in the
+// lane's registers (unrolled, so that register indices are constants); the
+// farther ones are one shuffle per 32-bit word, in a loop (the network
+// fully unrolled does not fit the instruction cache).  Ascending order.
+template <int E>
 __device__ static inline void warp_sort_events(uint64_t (&tb)[E], uint32_t (&ky)[E], uint32_t (&wv)[E],
                                                uint32_t lane) {
+  // merge steps k <= E: inside each lane's E registers
 #pragma unroll
-  for (int k = 2; k <= 32 * E; k <<= 1) {
+  for (int k = 2; k <= E; k <<= 1) {
+    if (k == 2) in_lane_stages<E, 1>(tb, ky, wv, lane, 2);
+    if (k == 4) in_lane_stages<E, 2>(tb, ky, wv, lane, 4);
+    if (k == 8) in_lane_stages<E, 4>(tb, ky, wv, lane, 8);
+  }
+  // merge steps k > E: exchanges across lanes down to distance E, then in-lane
+#pragma unroll 1
+  for (uint32_t k = 2 * E; k <= 32u * E; k <<= 1) {
+#pragma unroll 1
+    for (uint32_t j = k >> 1; j >= (uint32_t)E; j >>= 1) {
+      const uint32_t m = j / E;
+      const bool lower = (lane & m) == 0;
 #pragma unroll
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      if (j >= E) {
-        const int m = j / E;
-        const bool lower = (lane & (uint32_t)m) == 0;
-#pragma unroll
-        for (int r = 0; r < E; r++) {
-          const bool up = ((lane * E + r) & (uint32_t)k) == 0;
-          const uint32_t ylo = __shfl_xor_sync(0xffffffffu, (uint32_t)tb[r], m);
-          const uint32_t yhi = __shfl_xor_sync(0xffffffffu, (uint32_t)(tb[r] >> 32), m);
-          const uint32_t yk = __shfl_xor_sync(0xffffffffu, ky[r], m);
-          const uint32_t yw = __shfl_xor_sync(0xffffffffu, wv[r], m);
-          const uint64_t yt = ((uint64_t)yhi << 32) | ylo;
-          const bool x_lt_y = (tb[r] < yt) || (tb[r] == yt && ky[r] < yk);
-          // the lower position of an ascending pair keeps the smaller one
-          if ((lower == up) ? !x_lt_y : x_lt_y) {
-            tb[r] = yt;
-            ky[r] = yk;
-            wv[r] = yw;
-          }
-        }
-      } else {
-#pragma unroll
-        for (int r = 0; r < E; r++) {
-          if (r & j) continue;
-          const int q = r | j;
-          const bool up = ((lane * E + r) & (uint32_t)k) == 0;
-          const bool gt = (tb[r] > tb[q]) || (tb[r] == tb[q] && ky[r] > ky[q]);
-          if (gt == up) {
-            const uint64_t t0 = tb[r];
-            tb[r] = tb[q];
-            tb[q] = t0;
-            const uint32_t k0 = ky[r];
-            ky[r] = ky[q];
-            ky[q] = k0;
-            const uint32_t w0 = wv[r];
-            wv[r] = wv[q];
-            wv[q] = w0;
-          }
+      for (int r = 0; r < E; r++) {
+        const bool up = ((lane * E + r) & k) == 0;
+        const uint32_t ylo = __shfl_xor_sync(0xffffffffu, (uint32_t)tb[r], m);
+        const uint32_t yhi = __shfl_xor_sync(0xffffffffu, (uint32_t)(tb[r] >> 32), m);
+        const uint32_t yk = __shfl_xor_sync(0xffffffffu, ky[r], m);
+        const uint32_t yw = __shfl_xor_sync(0xffffffffu, wv[r], m);
+        const uint64_t yt = ((uint64_t)yhi << 32) | ylo;
+        const bool x_lt_y = (tb[r] < yt) || (tb[r] == yt && ky[r] < yk);
+        // the lower position of an ascending pair keeps the smaller one
+        if ((lower == up) ? !x_lt_y : x_lt_y) {
+          tb[r] = yt;
+          ky[r] = yk;
+          wv[r] = yw;
         }
       }
     }
+    in_lane_stages<E, E / 2>(tb, ky, wv, lane, k);
   }
 }
 
@@ -1426,7 +1651,7 @@ __device__ static inline void heavy_sort_one(const Dev &d, uint2 *ev, uint32_t n
 
 // A warp per neuron of the warp path (LOCAL_EVENTS < n <= HEAVY_WARP_MAX):
 // registers only, no shared memory.
-__global__ void __launch_bounds__(HEAVY_SORT_THREADS, 4) heavy_sort_kernel(Dev d) {
+__global__ void __launch_bounds__(HEAVY_SORT_THREADS, 2) heavy_sort_kernel(Dev d) {
   const NetConst *net = d.net;
   const uint32_t t = *d.t, N = net->N, D = net->D, cap = net->ev_cap, wmax = warp_path_max(net);
   const uint32_t lane = threadIdx.x & 31;
@@ -1611,6 +1836,9 @@ __global__ void ltp_kernel(Dev d) {
   }
 }
 
+// After each bath launch, on the bath stream: the next bath's step.
+__global__ void bath_tick_kernel(Dev d) { *d.bath_t = *d.bath_t + 1; }
+
 __global__ void end_step_kernel(Dev d) {
   *d.ovf_cnt = 0;
   d.heavy_cnt[0] = 0;
@@ -1704,8 +1932,11 @@ struct dpsnn_engine {
   std::vector<uint64_t> h_row;     // host copies of the CSR row and delay offsets
   std::vector<uint16_t> h_so;      // (for the STDP event log's order)
   std::vector<void *> allocs;
+  std::vector<void *> temps;       // build scratch, released when the build ends
+  uint64_t bytes = 0;              // device memory held (allocs)
   uint32_t grid_neuron = 0, grid_deliver = 0, grid_heavy = 0, grid_heavy_run = 0, grid_huge = 0;
   int timing = 0;
+  bool capturing = false;          // steps are being recorded into a graph
   struct TimedLaunch { int family; cudaEvent_t a, b; cudaStream_t st; };
   std::vector<TimedLaunch> pending;   // recorded, not yet read
   std::vector<cudaEvent_t> event_pool;
@@ -1723,18 +1954,22 @@ struct dpsnn_engine {
 
 static void collect_timings(dpsnn_engine *e);
 
+// Device allocations are stream-ordered on the engine stream (the
+// device's memory pool): unlike cudaMalloc/cudaFree they do not synchronise
+// the device, so engines built from several host threads, or while other
+// engines step, do not wait for each other.  `temp` allocations (the
+// connectome build's scratch) are released at the end of the build.
 template <typename T>
-static int dalloc(dpsnn_engine *e, T **p, size_t n, bool zero = true) {
+static int dalloc(dpsnn_engine *e, T **p, size_t n, bool temp = false) {
   void *q = nullptr;
   size_t bytes = std::max<size_t>(n * sizeof(T), 16);
-  cudaError_t err = cudaMalloc(&q, bytes);
+  cudaError_t err = cudaMallocAsync(&q, bytes, e->stream);
   if (err != cudaSuccess)
-    return dpsnn_fail(DPSNN_E_NOMEM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(err));
-  e->allocs.push_back(q);
-  if (zero) {
-    err = cudaMemsetAsync(q, 0, bytes, e->stream);
-    if (err != cudaSuccess) return dpsnn_fail(DPSNN_E_CUDA, "cudaMemset: %s", cudaGetErrorString(err));
-  }
+    return dpsnn_fail(DPSNN_E_NOMEM, "cudaMallocAsync(%zu bytes): %s", bytes, cudaGetErrorString(err));
+  (temp ? e->temps : e->allocs).push_back(q);
+  if (!temp) e->bytes += bytes;
+  err = cudaMemsetAsync(q, 0, bytes, e->stream);
+  if (err != cudaSuccess) return dpsnn_fail(DPSNN_E_CUDA, "cudaMemsetAsync: %s", cudaGetErrorString(err));
   *p = (T *)q;
   return 0;
 }
@@ -1743,6 +1978,16 @@ static int dalloc(dpsnn_engine *e, T **p, size_t n, bool zero = true) {
     int rc_ = dalloc(e, &(ptr), (size_t)(n));   \
     if (rc_) return rc_;                        \
   } while (0)
+#define TALLOC(ptr, n)                                \
+  do {                                                \
+    int rc_ = dalloc(e, &(ptr), (size_t)(n), true);   \
+    if (rc_) return rc_;                              \
+  } while (0)
+
+static void free_temps(dpsnn_engine *e) {
+  for (void *q : e->temps) cudaFreeAsync(q, e->stream);
+  e->temps.clear();
+}
 
 static int load_logf_fixup(dpsnn_engine *e) {
   std::string path = std::string(dpsnn_library_dir()) + "/logf_fixup.bin";
@@ -1959,7 +2204,7 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
             at(M - x, M - y) = v;
             at(M + x, M - y) = v;
           }
-    DALLOC(dprob, prob.size());
+    TALLOC(dprob, prob.size());
     CK(cudaMemcpyAsync(dprob, prob.data(), prob.size() * sizeof(float), cudaMemcpyHostToDevice, e->stream));
     CK(cudaStreamSynchronize(e->stream));
   }
@@ -1978,21 +2223,23 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
   GenRecord *drec;
   uint16_t *cnt_out;
   uint32_t *scratch;
-  DALLOC(drec, 2 * nmod);
-  DALLOC(cnt_out, 2ull * N * D);
+  TALLOC(drec, 2 * nmod);
+  TALLOC(cnt_out, 2ull * N * D);
   const uint32_t SD = p->stencil_dim;
   uint32_t *bath_tmpl;
   {
-    DALLOC(scratch, (size_t)2 * nmod * MAX_SYN_PER_NEURON);
-    DALLOC(bath_tmpl, SD * SD);
+    TALLOC(scratch, (size_t)2 * nmod * MAX_SYN_PER_NEURON);
+    TALLOC(bath_tmpl, SD * SD);
     std::vector<uint32_t> bath(p->bath, p->bath + SD * SD);
     CK(cudaMemcpyAsync(bath_tmpl, bath.data(), 4ull * SD * SD, cudaMemcpyHostToDevice, e->stream));
   }
   int32_t *dhyp;
   double *dcache;
-  DALLOC(dhyp, nmod);
-  DALLOC(dcache, nmod);
-  gen_kernel<<<(2 * nmod + 63) / 64, 64, 0, e->stream>>>(d.net, dprob, 0, drec, dhyp, dcache, cnt_out,
+  TALLOC(dhyp, nmod);
+  TALLOC(dcache, nmod);
+  CK(cudaFuncSetAttribute(gen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEN_SMEM));
+  gen_kernel<<<(2 * nmod + GEN_THREADS - 1) / GEN_THREADS, GEN_THREADS, GEN_SMEM, e->stream>>>(
+      d.net, dprob, 0, drec, dhyp, dcache, cnt_out,
                                                           nullptr, nullptr, nullptr, nullptr, scratch,
                                                           bath_tmpl, nullptr, nullptr, nullptr);
   CK(cudaGetLastError());
@@ -2042,7 +2289,7 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
   // ---- CSR offsets from the chosen counts
   uint32_t *row_len;
   DALLOC(d.sub_off, (size_t)N * (D + 1));
-  DALLOC(row_len, N);
+  TALLOC(row_len, N);
   counts_to_csr_kernel<<<(N + 255) / 256, 256, 0, e->stream>>>(d.net, cnt_out, dhyp, d.sub_off, row_len);
   CK(cudaGetLastError());
   std::vector<uint32_t> hlen(N);
@@ -2057,7 +2304,8 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
   DALLOC(d.post, e->S);
   DALLOC(d.w16, e->S);
   // ---- pass B: regenerate the chosen hypothesis straight into the CSR
-  gen_kernel<<<(nmod + 63) / 64, 64, 0, e->stream>>>(d.net, dprob, 1, drec, dhyp, dcache, cnt_out, d.row_ptr,
+  gen_kernel<<<(nmod + GEN_THREADS - 1) / GEN_THREADS, GEN_THREADS, GEN_SMEM, e->stream>>>(
+      d.net, dprob, 1, drec, dhyp, dcache, cnt_out, d.row_ptr,
                                                       d.sub_off, d.post, d.w16, scratch, bath_tmpl, d.inv_nu,
                                                       d.max_ext, d.sub);
   CK(cudaGetLastError());
@@ -2066,18 +2314,14 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
   CK(cudaStreamSynchronize(e->stream));
   for (uint32_t m = 0; m < nmod; m++)
     if (recB[m].err) return dpsnn_fail(DPSNN_E_MODEL, "synapse generation pass B error %d", recB[m].err);
-  // The generation scratch (cnt_out, scratch, row_len, bath_tmpl) stays
-  // allocated until dpsnn_destroy: cudaFree waits for the whole device, so
-  // freeing here would serialise builds issued from several host threads
-  // behind each other's generation kernels.
   // ---- run-over-group-end check (see DPSNN_synapse.c:211-265): the reference's
   // search continues past a (delay, source rank) group while the next entry has
   // the same presynaptic index; this happens only when the last source of a
   // delay group is also the first source of the next non-empty group.
   {
     uint32_t *gmax, *gmin;
-    DALLOC(gmax, (size_t)P * D);
-    DALLOC(gmin, (size_t)P * D);
+    TALLOC(gmax, (size_t)P * D);
+    TALLOC(gmin, (size_t)P * D);
     CK(cudaMemsetAsync(gmin, 0xFF, 4ull * P * D, e->stream));
     group_extrema_kernel<<<std::min<uint32_t>(4096, (N + 7) / 8), 256, 0, e->stream>>>(d.net, d.row_ptr,
                                                                                      d.sub_off, d.post, gmax, gmin);
@@ -2099,13 +2343,16 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
       }
   }
   // ---- STDP arrays
+  if (n.stdp_on && e->S > 0xFFFFFFFFull)   // in_idx holds 32-bit synapse indices
+    return dpsnn_fail(DPSNN_E_CAPACITY, "plasticity supports at most 2^32-1 synapses (%llu generated)",
+                      (unsigned long long)e->S);
   if (n.stdp_on) {
     DALLOC(d.tderiv, e->S);
     DALLOC(d.last_act, e->S);
     DALLOC(d.in_ptr, N + 1);
     DALLOC(d.in_idx, e->S);
     unsigned long long *fill;
-    DALLOC(fill, N);
+    TALLOC(fill, N);
     in_count_kernel<<<2048, 256, 0, e->stream>>>(d.net, d.post, e->S, d.in_ptr);
     CK(cudaGetLastError());
     std::vector<uint64_t> ip(N + 1);
@@ -2131,6 +2378,7 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
   DALLOC(d.heavy_list, 4ull * N);
   DALLOC(d.heavy_cnt, 2);
   DALLOC(d.t, 1);
+  DALLOC(d.bath_t, 1);
   DALLOC(d.flags, 4);
   DALLOC(d.events, 1);
   init_neurons_kernel<<<(N + 255) / 256, 256, 0, e->stream>>>(d);
@@ -2212,7 +2460,6 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
   }
   int rc = load_logf_fixup(e);
   if (rc) return rc;
-  // dprob too stays allocated until dpsnn_destroy (no device-wide cudaFree)
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
   e->grid_deliver = (uint32_t)sms * 8;
@@ -2221,6 +2468,7 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
   e->grid_huge = (uint32_t)sms;
   CK(cudaFuncSetAttribute(bath_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(BathSmem)));
   CK(cudaFuncSetAttribute(huge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, HEAVY_SMEM));
+  free_temps(e);   // after their last use on this stream
   CK(cudaStreamSynchronize(e->stream));
   return 0;
 }
@@ -2265,9 +2513,13 @@ extern "C" int dpsnn_create(const dpsnn_params *p, const dpsnn_options *opts, dp
 extern "C" void dpsnn_destroy(dpsnn_engine *e) {
   if (!e) return;
   cudaSetDevice(e->device);
-  if (e->stream) cudaStreamSynchronize(e->stream);
   if (e->bath_stream) cudaStreamSynchronize(e->bath_stream);
-  for (void *q : e->allocs) cudaFree(q);
+  if (e->read_stream) cudaStreamSynchronize(e->read_stream);
+  if (e->stream) {
+    free_temps(e);   // a build that stopped early
+    for (void *q : e->allocs) cudaFreeAsync(q, e->stream);
+    cudaStreamSynchronize(e->stream);
+  }
   collect_timings(e);
   for (cudaEvent_t ev : e->event_pool) cudaEventDestroy(ev);
   for (int b = 0; b < 2; b++) {
@@ -2362,7 +2614,9 @@ static void enqueue_bath(dpsnn_engine *e, uint32_t t) {
   db.bath_cnt = e->bath_cnt2[b];
   cudaStreamWaitEvent(e->bath_stream, e->ev_neuron[b], 0);
   timed_launch_begin(e, 2, e->bath_stream);
-  bath_kernel<<<e->hnet.P, BATH_THREADS, sizeof(BathSmem), e->bath_stream>>>(db, t);
+  // the kernel reads its step from d.bath_t (baths are launched in step order)
+  bath_kernel<<<e->hnet.P, BATH_THREADS, sizeof(BathSmem), e->bath_stream>>>(db);
+  bath_tick_kernel<<<1, 1, 0, e->bath_stream>>>(db);
   timed_launch_end(e, 2);
   cudaEventRecord(e->ev_bath[b], e->bath_stream);
 }
@@ -2375,6 +2629,7 @@ static int enqueue_step(dpsnn_engine *e) {
     cudaStreamWaitEvent(e->bath_stream, e->ev_start, 0);
     enqueue_bath(e, t);
     e->bath_primed = true;
+    e->launches += 2;
   }
   enqueue_bath(e, t + 1);
   if (e->d.stdp_log) {
@@ -2389,7 +2644,11 @@ static int enqueue_step(dpsnn_engine *e) {
   timed_launch_begin(e, 0);
   compact_kernel<<<e->grid_neuron, NEURON_BLOCK, 0, e->stream>>>(d);
   timed_launch_end(e, 0);
-  cudaEventRecord(e->ev_slot[t % RING_SLOTS], e->stream);   // slot t is final
+  // slot t is final (inside a graph: an event the graph records on every run)
+  if (e->capturing)
+    cudaEventRecordWithFlags(e->ev_slot[t % RING_SLOTS], e->stream, cudaEventRecordExternal);
+  else
+    cudaEventRecord(e->ev_slot[t % RING_SLOTS], e->stream);
   if (e->hnet.stdp_on) {
     timed_launch_begin(e, 4);
     causal_stdp_kernel<<<e->grid_deliver, 256, 0, e->stream>>>(d);
@@ -2423,7 +2682,7 @@ static int enqueue_step(dpsnn_engine *e) {
     timed_launch_end(e, 4);
   }
   end_step_kernel<<<1, 1, 0, e->stream>>>(d);
-  e->launches += 8 + (e->hnet.stdp_on ? 2 : 0);
+  e->launches += 9 + (e->hnet.stdp_on ? 2 : 0);
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) return dpsnn_fail(DPSNN_E_CUDA, "kernel launch: %s", cudaGetErrorString(err));
   e->t_host++;
@@ -2453,6 +2712,142 @@ extern "C" int dpsnn_step_many(dpsnn_engine *const *engines, uint32_t n, uint32_
       int rc = enqueue_step(e);
       if (rc) return rc;
     }
+  return 0;
+}
+
+// ------------------------------------------------------------------ graphs of batched steps
+// nsteps steps of n engines queued as dpsnn_step_many does, recorded once into
+// a CUDA graph and run as one launch: the host cost of a step of many small
+// networks (a dozen launches and event operations per network) is paid once.
+// A graph encodes the engines' ring slots and step parities, so it runs only
+// when every engine is at the step (mod 80) it was recorded at; nsteps is a
+// multiple of 80, so consecutive runs chain.
+struct dpsnn_graph {
+  std::vector<dpsnn_engine *> engines;
+  std::vector<uint32_t> t0;        // each engine's step (mod RING_SLOTS) at recording
+  std::vector<cudaEvent_t> pre;    // per engine: its two streams' last work before a run
+  uint32_t nsteps = 0;
+  uint64_t launches_per_run = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t fork = nullptr, done = nullptr;
+};
+
+extern "C" void dpsnn_graph_destroy(dpsnn_graph *g) {
+  if (!g) return;
+  cudaSetDevice(g->device);
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  for (cudaEvent_t ev : g->pre) cudaEventDestroy(ev);
+  if (g->fork) cudaEventDestroy(g->fork);
+  if (g->done) cudaEventDestroy(g->done);
+  if (g->stream) cudaStreamDestroy(g->stream);
+  delete g;
+}
+
+extern "C" int dpsnn_graph_create(dpsnn_engine *const *engines, uint32_t n, uint32_t nsteps, dpsnn_graph **out) {
+  if (!out || (!engines && n)) return dpsnn_fail(DPSNN_E_PARAM, "null argument");
+  *out = nullptr;
+  if (n == 0 || nsteps == 0 || nsteps % RING_SLOTS)
+    return dpsnn_fail(DPSNN_E_PARAM, "a graph holds a positive multiple of %d steps of at least one engine",
+                      RING_SLOTS);
+  for (uint32_t i = 0; i < n; i++) {
+    const dpsnn_engine *e = engines[i];
+    if (!e) return dpsnn_fail(DPSNN_E_PARAM, "null engine %u", i);
+    if (e->device != engines[0]->device) return dpsnn_fail(DPSNN_E_PARAM, "engines on different devices");
+    if (!e->bath_primed) return dpsnn_fail(DPSNN_E_STATE, "engine %u has not run its first step", i);
+    if (e->timing || e->d.stdp_log || e->d.probe_w)
+      return dpsnn_fail(DPSNN_E_STATE, "engine %u has kernel timing, the STDP event log or the LTP probe on", i);
+    for (uint32_t k = 0; k < i; k++)
+      if (engines[k] == e) return dpsnn_fail(DPSNN_E_PARAM, "engine %u is listed twice", i);
+  }
+  dpsnn_graph *g = new dpsnn_graph();
+  g->device = engines[0]->device;
+  g->nsteps = nsteps;
+  g->engines.assign(engines, engines + n);
+  cudaSetDevice(g->device);
+  auto fail = [&](int rc) {
+    dpsnn_graph_destroy(g);
+    return rc;
+  };
+  if (cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&g->done, cudaEventDisableTiming) != cudaSuccess)
+    return fail(dpsnn_fail(DPSNN_E_CUDA, "cannot create the graph's stream and events"));
+  g->pre.resize(2 * n, nullptr);
+  for (auto &ev : g->pre)
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+      return fail(dpsnn_fail(DPSNN_E_CUDA, "cannot create the graph's events"));
+  std::vector<uint32_t> t_saved(n);
+  std::vector<uint64_t> l_saved(n);
+  cudaError_t err = cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal);
+  if (err != cudaSuccess) return fail(dpsnn_fail(DPSNN_E_CUDA, "cudaStreamBeginCapture: %s", cudaGetErrorString(err)));
+  cudaEventRecord(g->fork, g->stream);
+  int rc = 0;
+  for (uint32_t i = 0; i < n; i++) {
+    dpsnn_engine *e = engines[i];
+    t_saved[i] = e->t_host;
+    l_saved[i] = e->launches;
+    g->t0.push_back(e->t_host % RING_SLOTS);
+    // both streams join the recording; the events they wait on between
+    // each other are recorded inside it from here on
+    cudaStreamWaitEvent(e->stream, g->fork, 0);
+    cudaStreamWaitEvent(e->bath_stream, g->fork, 0);
+    for (int b = 0; b < 2; b++) {
+      cudaEventRecord(e->ev_neuron[b], e->stream);
+      cudaEventRecord(e->ev_bath[b], e->bath_stream);
+    }
+    e->capturing = true;
+  }
+  for (uint32_t k = 0; k < nsteps && !rc; k++)
+    for (uint32_t i = 0; i < n && !rc; i++) rc = enqueue_step(engines[i]);
+  for (uint32_t i = 0; i < n; i++) {
+    dpsnn_engine *e = engines[i];
+    e->capturing = false;
+    cudaEventRecord(g->pre[2 * i], e->stream);
+    cudaEventRecord(g->pre[2 * i + 1], e->bath_stream);
+    cudaStreamWaitEvent(g->stream, g->pre[2 * i], 0);
+    cudaStreamWaitEvent(g->stream, g->pre[2 * i + 1], 0);
+    g->launches_per_run += e->launches - l_saved[i];
+    e->t_host = t_saved[i];   // nothing ran
+    e->launches = l_saved[i];
+  }
+  err = cudaStreamEndCapture(g->stream, &g->graph);
+  if (rc) return fail(rc);
+  if (err != cudaSuccess) return fail(dpsnn_fail(DPSNN_E_CUDA, "cudaStreamEndCapture: %s", cudaGetErrorString(err)));
+  err = cudaGraphInstantiate(&g->exec, g->graph, 0);
+  if (err != cudaSuccess) return fail(dpsnn_fail(DPSNN_E_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(err)));
+  *out = g;
+  return 0;
+}
+
+extern "C" int dpsnn_graph_run(dpsnn_graph *g) {
+  if (!g) return dpsnn_fail(DPSNN_E_PARAM, "null graph");
+  cudaSetDevice(g->device);
+  const uint32_t n = (uint32_t)g->engines.size();
+  for (uint32_t i = 0; i < n; i++)
+    if (g->engines[i]->t_host % RING_SLOTS != g->t0[i])
+      return dpsnn_fail(DPSNN_E_STATE, "engine %u is at step %u; the graph was recorded at a step = %u (mod %d)", i,
+                        g->engines[i]->t_host, g->t0[i], RING_SLOTS);
+  for (uint32_t i = 0; i < n; i++) {   // after the engines' queued work
+    dpsnn_engine *e = g->engines[i];
+    CK(cudaEventRecord(g->pre[2 * i], e->stream));
+    CK(cudaEventRecord(g->pre[2 * i + 1], e->bath_stream));
+    CK(cudaStreamWaitEvent(g->stream, g->pre[2 * i], 0));
+    CK(cudaStreamWaitEvent(g->stream, g->pre[2 * i + 1], 0));
+  }
+  CK(cudaGraphLaunch(g->exec, g->stream));
+  CK(cudaEventRecord(g->done, g->stream));
+  for (uint32_t i = 0; i < n; i++) {   // later work on the engines' streams follows the graph
+    dpsnn_engine *e = g->engines[i];
+    CK(cudaStreamWaitEvent(e->stream, g->done, 0));
+    CK(cudaStreamWaitEvent(e->bath_stream, g->done, 0));
+    e->t_host += g->nsteps;
+  }
+  g->engines[0]->launches += g->launches_per_run;   // counted on the first engine
   return 0;
 }
 
@@ -2503,6 +2898,45 @@ extern "C" int dpsnn_spikes(dpsnn_engine *e, uint32_t t_ms, uint32_t *ids, doubl
   if (k && (ids || te)) CK(cudaStreamSynchronize(e->read_stream));
   return 0;
 }
+
+extern "C" int dpsnn_spikes_range(dpsnn_engine *e, uint32_t t0, uint32_t n, uint32_t *ids, double *te,
+                                  uint64_t cap, uint32_t *counts) {
+  if (!e || !counts || (n && (!ids || !te))) return dpsnn_fail(DPSNN_E_PARAM, "null argument");
+  if (n == 0) return 0;
+  if (n > RING_SLOTS || t0 + n > e->t_host || t0 + RING_SLOTS <= e->t_host)
+    return dpsnn_fail(DPSNN_E_STATE, "steps %u..%u are not among the last %d completed steps", t0, t0 + n - 1,
+                      RING_SLOTS);
+  cudaSetDevice(e->device);
+  // after the compaction of the last step of the run (steps complete in
+  // order on the engine stream): the counts and the error flags, then the lists
+  CK(cudaStreamWaitEvent(e->read_stream, e->ev_slot[(t0 + n - 1) % RING_SLOTS], 0));
+  CK(cudaMemcpyAsync(e->h_pin, e->d.flags, 4, cudaMemcpyDeviceToHost, e->read_stream));
+  for (uint32_t k = 0; k < n; k++)
+    CK(cudaMemcpyAsync(counts + k, e->d.ring_cnt + (t0 + k) % RING_SLOTS, 4, cudaMemcpyDeviceToHost,
+                       e->read_stream));
+  CK(cudaStreamSynchronize(e->read_stream));
+  int rc = flags_error(e->h_pin[0]);
+  if (rc) return rc;
+  uint64_t off = 0;
+  for (uint32_t k = 0; k < n; k++) off += counts[k];
+  if (off > cap) return dpsnn_fail(DPSNN_E_CAPACITY, "%llu spikes in steps %u..%u exceed the buffers (%llu)",
+                                   (unsigned long long)off, t0, t0 + n - 1, (unsigned long long)cap);
+  off = 0;
+  for (uint32_t k = 0; k < n; k++) {
+    const size_t slot = (t0 + k) % RING_SLOTS;
+    if (counts[k]) {
+      CK(cudaMemcpyAsync(ids + off, e->d.ring_ids + slot * e->hnet.N, 4ull * counts[k], cudaMemcpyDeviceToHost,
+                         e->read_stream));
+      CK(cudaMemcpyAsync(te + off, e->d.ring_te + slot * e->hnet.N, 8ull * counts[k], cudaMemcpyDeviceToHost,
+                         e->read_stream));
+    }
+    off += counts[k];
+  }
+  CK(cudaStreamSynchronize(e->read_stream));
+  return 0;
+}
+
+extern "C" uint64_t dpsnn_device_bytes(const dpsnn_engine *e) { return e ? e->bytes : 0; }
 
 extern "C" int dpsnn_state(dpsnn_engine *e, double *v, double *c, double *tr, double *te, double *nb) {
   if (!e) return dpsnn_fail(DPSNN_E_PARAM, "null engine");
@@ -2807,26 +3241,30 @@ extern "C" int dpsnn_rank_spikes_noalloc(dpsnn_engine *e, uint32_t t_ms, uint32_
   if (e->hnet.locN > DPSNN_NOALLOC_MAX_SPIKES)
     return dpsnn_fail(DPSNN_E_CAPACITY, "rank of %u neurons exceeds the %d-spike scratch of dpsnn_rank_spikes_noalloc",
                       e->hnet.locN, DPSNN_NOALLOC_MAX_SPIKES);
-  cudaSetDevice(e->device);
-  int rc = dpsnn_sync(e);
-  if (rc) return rc;
   if (t_ms >= e->t_host || t_ms + RING_SLOTS <= e->t_host)
     return dpsnn_fail(DPSNN_E_STATE, "step %u is not among the last %d completed steps", t_ms, RING_SLOTS);
+  cudaSetDevice(e->device);
   NoAllocScratch *s = nullptr;
-  rc = noalloc_scratch(e->device, &s);
+  int rc = noalloc_scratch(e->device, &s);
   if (rc) return rc;
   const uint32_t slot = t_ms % RING_SLOTS;
   const size_t off = (size_t)slot * e->hnet.N;
-  rank_select_kernel<<<1, 256, 0, e->stream>>>(e->d.ring_ids + off, e->d.ring_te + off, e->d.ring_cnt + slot,
-                                               h * e->hnet.locN, (h + 1) * e->hnet.locN, s);
+  // on the read stream, after the compaction of step t_ms only (as
+  // dpsnn_spikes): later steps keep running on the engine stream
+  CK(cudaStreamWaitEvent(e->read_stream, e->ev_slot[slot], 0));
+  rank_select_kernel<<<1, 256, 0, e->read_stream>>>(e->d.ring_ids + off, e->d.ring_te + off, e->d.ring_cnt + slot,
+                                                    h * e->hnet.locN, (h + 1) * e->hnet.locN, s);
   CK(cudaGetLastError());
-  uint32_t n = 0;
-  CK(cudaMemcpyAsync(&n, &s->count, 4, cudaMemcpyDeviceToHost, e->stream));
-  CK(cudaStreamSynchronize(e->stream));
+  CK(cudaMemcpyAsync(e->h_pin, e->d.flags, 4, cudaMemcpyDeviceToHost, e->read_stream));
+  CK(cudaMemcpyAsync(e->h_pin + 1, &s->count, 4, cudaMemcpyDeviceToHost, e->read_stream));
+  CK(cudaStreamSynchronize(e->read_stream));
+  rc = flags_error(e->h_pin[0]);
+  if (rc) return rc;
+  const uint32_t n = e->h_pin[1];
   *count = n;
   const uint32_t k = std::min(n, cap);
-  if (k && ids) CK(cudaMemcpyAsync(ids, s->ids, 4ull * k, cudaMemcpyDeviceToHost, e->stream));
-  if (k && te) CK(cudaMemcpyAsync(te, s->te, 8ull * k, cudaMemcpyDeviceToHost, e->stream));
-  CK(cudaStreamSynchronize(e->stream));
+  if (k && ids) CK(cudaMemcpyAsync(ids, s->ids, 4ull * k, cudaMemcpyDeviceToHost, e->read_stream));
+  if (k && te) CK(cudaMemcpyAsync(te, s->te, 8ull * k, cudaMemcpyDeviceToHost, e->read_stream));
+  if (k && (ids || te)) CK(cudaStreamSynchronize(e->read_stream));
   return 0;
 }

@@ -57,6 +57,7 @@ EXPORTS = [
     "dpsnn_bath_params", "dpsnn_set_timing", "dpsnn_kernel_times", "dpsnn_kernel_launches", "dpsnn_cuda_stream",
     "dpsnn_rank_spikes_noalloc", "dpsnn_enable_ltp_probe", "dpsnn_ltp_probe",
     "dpsnn_enable_stdp_events", "dpsnn_stdp_events", "dpsnn_step_many", "dpsnn_last_error",
+    "dpsnn_spikes_range", "dpsnn_device_bytes",
 ]
 NOALLOC_MAX_SPIKES = 32768   # DPSNN_NOALLOC_MAX_SPIKES
 TIMING_SLOTS = 8             # DPSNN_TIMING_SLOTS
@@ -108,6 +109,9 @@ def load_library(path: str = LIB_PATH):
     lib.dpsnn_enable_stdp_events.argtypes = [P]
     lib.dpsnn_stdp_events.argtypes = [P, C.POINTER(C.c_uint32), P, P, P, C.c_uint32, C.POINTER(C.c_uint32)]
     lib.dpsnn_step_many.argtypes = [P, C.c_uint32, C.c_uint32]
+    lib.dpsnn_spikes_range.argtypes = [P, C.c_uint32, C.c_uint32, P, P, C.c_uint64, P]
+    lib.dpsnn_device_bytes.argtypes = [P]
+    lib.dpsnn_device_bytes.restype = C.c_uint64
     lib.dpsnn_last_error.restype = C.c_char_p
     _LIB = lib
     return lib
@@ -229,6 +233,24 @@ class Engine:
                     "dpsnn_spikes")
         n = cnt.value
         return ids[:n].copy(), te[:n].copy()
+
+    def spikes_range(self, t0: int, n: int):
+        """(ids, emission times, per-step counts) of the spikes detected at
+        steps t0 .. t0+n-1, concatenated in step order (one wait)."""
+        cap = max(self.glob_n * n, 1)
+        if getattr(self, "_rbuf", None) is None or len(self._rbuf[0]) < cap:
+            self._rbuf = (np.empty(cap, np.uint32), np.empty(cap, np.float64))
+        ids, te = self._rbuf
+        counts = np.zeros(max(n, 1), np.uint32)
+        self._check(self._L.dpsnn_spikes_range(self._h, t0, n, _ptr(ids), _ptr(te), cap, _ptr(counts)),
+                    "dpsnn_spikes_range")
+        k = int(counts[:n].sum())
+        return ids[:k].copy(), te[:k].copy(), counts[:n]
+
+    @property
+    def device_bytes(self) -> int:
+        """Device memory the engine holds."""
+        return self._L.dpsnn_device_bytes(self._h)
 
     def rank_spikes_noalloc(self, t_ms: int, rank: int):
         """Spikes of one emulated rank at step t_ms, gathered without any

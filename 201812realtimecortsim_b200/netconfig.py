@@ -208,6 +208,8 @@ def lateral_p1_for_grid(cfx: int, cfy: int, stencil_dim: int = 2, lam: float = 1
                     if 0 <= sx < cfx and 0 <= sy < cfy:
                         tot += math.exp(-(math.hypot(dx, dy) - 1.0) / lam)
     mean_weight = tot / (cfx * cfy)
+    if mean_weight == 0:   # a single module: no lateral connections at all
+        return 0.0
     return lateral_indegree / (neurons_per_module * mean_weight)
 
 

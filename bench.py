@@ -164,9 +164,16 @@ def bench_network(args):
     nc = importlib.import_module("201812realtimecortsim_b200.netconfig")
     cfx, cfy = (int(x) for x in args.grid.lower().split("x"))
     total_ms = max(args.full_ms, args.warmup + args.steps + 10)
-    cfg = nc.cortical_grid(cfx, cfy, total_ms=total_ms, glob_h=args.ranks, delay_range_subpop=True)
-    workload = WORKLOAD if (cfx, cfy, args.ranks) == (24, 24, 192) else (
-        f"{cfx}x{cfy} grid, {cfg.glob_n} neurons, 1 ms steps, STDP off, RNG streams of {args.ranks} ranks")
+    cfg = nc.cortical_grid(cfx, cfy, total_ms=total_ms, glob_h=args.ranks, delay_range_subpop=True,
+                           stdp=args.stdp, start_plasticity_ms=0)
+    if args.stdp:
+        workload = (f"{cfx}x{cfy} grid, {cfg.glob_n} neurons, 1 ms steps, pair-based additive STDP on E->E "
+                    f"synapses from t=0 (A+ 0.01, A- 0.012, tau 20 ms, weights in [0, 2 mu], updated each s), "
+                    f"RNG streams of {args.ranks} ranks")
+    elif (cfx, cfy, args.ranks) == (24, 24, 192):
+        workload = WORKLOAD
+    else:
+        workload = f"{cfx}x{cfy} grid, {cfg.glob_n} neurons, 1 ms steps, STDP off, RNG streams of {args.ranks} ranks"
     return cfg, workload
 
 
@@ -366,6 +373,58 @@ def run_batch(args):
     }), flush=True)
 
 
+def run_serve(args):
+    """The served form (continuous batching) against the same jobs one at a
+    time: J jobs of the served-simulations stream (Poisson arrivals at 50/s,
+    1x1-16x16 modules log-uniform, 0.5-10 s of biological time scaled by
+    --serve-scale, 20 % with plasticity) under a 150 GB device-memory budget;
+    each arm on the same GPU, host wall time from the first arrival to the
+    last completion (builds included)."""
+    import numpy as np
+    S = importlib.import_module("201812realtimecortsim_b200.serve")
+
+    def stream():
+        jobs = S.poisson_jobs(args.serve, rate_per_s=50.0, seed=11)
+        for j in jobs:
+            j.duration_ms = max(1, int(round(j.duration_ms * args.serve_scale)))
+            j.cfg.total_ms = j.duration_ms + 1
+        return jobs
+
+    served = stream()
+    srv = S.Server(device=0, hbm_budget=150e9, max_slots=args.serve_slots, round_ms=40)
+    t0 = time.perf_counter()
+    srv.run(served)
+    t_served = time.perf_counter() - t0
+    # the same jobs one at a time: build, dpsnn_step through the duration
+    # with the spikes read back every 40 steps, release
+    alone = stream()
+    t0 = time.perf_counter()
+    S.run_one_at_a_time(alone, device=0, read_ms=40)
+    t_alone = time.perf_counter() - t0
+    ok = [j for j in served if not j.error]
+    lat = np.array([j.latency_s for j in ok])
+    rtf = np.array([j.real_time_factor for j in ok])
+    ev_s = sum(j.events for j in ok)
+    ev_a = sum(j.events for j in alone if not j.error)
+    print(json.dumps({
+        "metric": "aggregate synaptic events/s (served jobs)", "value": ev_s / t_served, "unit": UNIT,
+        "n_gpus": 1, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{len(served)} jobs: Poisson arrivals at 50/s, 1x1-16x16 modules (log-uniform), "
+                               f"0.5-10 s x {args.serve_scale} of biological time, 20% with STDP, one emulated "
+                               f"rank per module, 150 GB budget, {args.serve_slots} slots",
+                   "timing": "host wall time from the first arrival to the last completion, builds included"},
+        "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                      "max": float(lat.max())},
+        "real_time_factor": {"p50": float(np.percentile(rtf, 50)), "p99": float(np.percentile(rtf, 99))},
+        "served_s": t_served, "one_at_a_time_s": t_alone, "one_at_a_time_value": ev_a / t_alone,
+        "ratio_vs_one_at_a_time": (ev_s / t_served) / (ev_a / t_alone) if ev_a else None,
+        "results_identical_to_one_at_a_time": all(a.raster_sha256 == b.raster_sha256 and a.events == b.events
+                                                   for a, b in zip(served, alone) if not a.error),
+        "refused": [j.error for j in served if j.error],
+        "rounds": srv.rounds,
+    }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -378,12 +437,21 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", default="24x24", help="CFXxCFY modules (profiling of smaller grids)")
     ap.add_argument("--ranks", type=int, default=192, help="env_globH: emulated reference ranks")
+    ap.add_argument("--stdp", action="store_true",
+                    help="plasticity on (the 48x48 configuration: --grid 48x48 --ranks 256 --stdp)")
     ap.add_argument("--batch", type=int, default=0, help="run the batched sweep of this many networks instead")
+    ap.add_argument("--serve", type=int, default=0, help="run the served form with this many jobs instead")
+    ap.add_argument("--serve-scale", type=float, default=0.1,
+                    help="scale of the jobs' biological durations (a bounded sample)")
+    ap.add_argument("--serve-slots", type=int, default=64, help="jobs resident at once")
     ap.add_argument("--batch-ms", type=int, default=100,
                     help="biological ms per network timed in the batched sweep (a bounded sample)")
     args = ap.parse_args()
     if args.batch:
         run_batch(args)
+        return
+    if args.serve:
+        run_serve(args)
         return
     args.warmup = max(args.warmup, 3)
     world, rank, local, dist = dist_setup(args)

@@ -116,7 +116,9 @@ int dpsnn_step(dpsnn_engine *e, uint32_t nsteps);
 /* Batched form: nsteps steps of each of n independent engines, queued one
  * step of every engine at a time, so that their kernels overlap on the
  * device; each engine's results are those of dpsnn_step on it alone.
- * Asynchronous like dpsnn_step. */
+ * Asynchronous like dpsnn_step.  If queuing fails for engine i in round k,
+ * engines 0..i-1 have k+1 steps queued and engines i..n-1 have k:
+ * dpsnn_time_ms tells each engine's count. */
 int dpsnn_step_many(dpsnn_engine *const *engines, uint32_t n, uint32_t nsteps);
 /* Block until all queued steps are done; reports a deferred device error. */
 int dpsnn_sync(dpsnn_engine *e);
@@ -135,6 +137,18 @@ uint64_t dpsnn_events_delivered(const dpsnn_engine *e);
  * running; reports device errors raised so far. */
 int dpsnn_spikes(dpsnn_engine *e, uint32_t t_ms, uint32_t *ids, double *te,
                  uint32_t cap, uint32_t *count);
+
+/* Spike lists of the n consecutive steps t0 .. t0+n-1 (all among the last 80
+ * steps), concatenated in step order into ids/te (cap entries each), with
+ * counts[k] the spikes of step t0+k.  One wait for the whole run: for a
+ * caller collecting a raster every few tens of steps (the served form).  No
+ * counterpart in the reference, which writes each step's list to its spike
+ * file (DPSNN_stat.c:290). */
+int dpsnn_spikes_range(dpsnn_engine *e, uint32_t t0, uint32_t n, uint32_t *ids, double *te, uint64_t cap,
+                       uint32_t *counts);
+/* Device memory the engine holds (its network, state and buffers), for
+ * callers that budget device memory (admission of served jobs). */
+uint64_t dpsnn_device_bytes(const dpsnn_engine *e);
 
 /* Backward synapse list of rank h in the reference's memory order (sorted by
  * delay, source rank, generation order), as dumped by synapticListReport.
@@ -204,10 +218,13 @@ void *dpsnn_cuda_stream(const dpsnn_engine *e);
  * a host that budgets every byte of device memory itself.  The gather goes
  * through a fixed scratch area in the library image holding
  * DPSNN_NOALLOC_MAX_SPIKES spikes (384 KiB); engines whose ranks hold more
- * neurons get DPSNN_E_CAPACITY.  There is one scratch per device and process:
- * calls that overlap in time on the same device (from several threads, or
- * several engines on one device) race on it and must be serialised by the
- * caller. */
+ * neurons get DPSNN_E_CAPACITY.  Like dpsnn_spikes it waits only for the
+ * compaction of step t_ms, so later queued steps keep running.  The first
+ * call on a device looks up the scratch's device address (once per device),
+ * so that call should come before any stream capture.  There is one scratch
+ * per device and process: calls that overlap in time on the same device
+ * (from several threads, or several engines on one device) race on it and
+ * must be serialised by the caller. */
 #define DPSNN_NOALLOC_MAX_SPIKES 32768
 int dpsnn_rank_spikes_noalloc(dpsnn_engine *e, uint32_t t_ms, uint32_t h, uint32_t *ids, double *te,
                               uint32_t cap, uint32_t *count);

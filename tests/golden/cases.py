@@ -48,6 +48,12 @@ SUMMARY_CASES = {
                       (0,), (1000, 10000)),
     # the 2x2 benchmark network, 1 rank, 10 s
     "c1_2x2_10s": (lambda: nc.cortical_grid(2, 2, total_ms=10000), (0,), (1000, 10000)),
+    # the plasticity configuration on a 4x4 subgrid (20000 neurons, 1 rank):
+    # pair-based additive STDP on E->E synapses (A+ 0.01, A- 0.012, tau 20 ms,
+    # weights clipped to [0, 2 mu], updated each second) from t = 0, through
+    # two weight updates (ms 999 and 1999)
+    "c3_4x4_stdp": (lambda: nc.cortical_grid(4, 4, total_ms=2100, stdp=True, start_plasticity_ms=0,
+                                             delay_range_subpop=True), (0,), (1000, 2100)),
 }
 
 

@@ -1,7 +1,8 @@
 """dpsnn_rank_spikes_noalloc against dpsnn_spikes: the same rank's spike
 list on two calls in a row, for every rank and for consecutive steps; ranks
-larger than the fixed scratch are rejected.  Collected last (file name), and
-independent of the tests before it."""
+larger than the fixed scratch are rejected; calls leave the device's free
+memory unchanged.  Collected last (file name), and independent of the tests
+before it."""
 import numpy as np
 import pytest
 
@@ -59,4 +60,25 @@ def test_rejects_rank_larger_than_scratch():
     eng.step(1)
     with pytest.raises(E.EngineError, match="exceeds the 32768-spike scratch"):
         eng.rank_spikes_noalloc(0, 0)
+    eng.close()
+
+
+def test_device_memory_unchanged_over_many_calls():
+    """No call allocates: the device's free memory is the same before and
+    after 100 calls (after a first call, which looks up the scratch address,
+    and with the engine's queued work finished)."""
+    import torch
+    cfg = CASES["small_2x2"]()
+    cfg.glob_h = 4
+    eng = E.Engine(cfg)
+    eng.step(40)
+    eng.sync()
+    eng.rank_spikes_noalloc(39, 0)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    for k in range(100):
+        eng.rank_spikes_noalloc(39 - (k % 40), k % 4)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0
     eng.close()
