@@ -704,32 +704,38 @@ __global__ void __launch_bounds__(DELIVER_THREADS) deliver_kernel(Dev d) {
 // rank runs a shared-memory pipeline:
 //   warp 1     extends the lagged Fibonacci sequence 24 values per round
 //              (x[n] = x[n-55] - x[n-24] mod 1e9) into a ring of raw draws;
-//   warps 2,3,5,6,7 convert each round into the LUT index (uint32)(u*256) and the
-//              lapse factor -logf((float)(1-u)), and extend q[], the running
-//              sum over draws of one parity of the lapses in 2^-20 units
-//              (q[n] = q[n-2] + round(lap[n] * 2^20), integers mod 2^32);
-//   warps 4, 8 stay idle: warps go to the SM's four schedulers by index, so
-//              this leaves warp 0 a scheduler of its own;
-//   warps 5-7, 9-11 tabulate the event counts of the next chunk of 32
-//              neurons.  The number of events c of a neuron is the first c
-//              at which nextBath + sum of c lapses * invNuExt reaches t+1; it
-//              depends on where in the stream the neuron starts, which is
-//              known only once every earlier neuron of the rank is decided.
-//              Each lane turns its neuron's budget (t+1 - nextBath)/invNuExt
-//              into two integer bounds that enclose every rounding of the
-//              reference's sequential sum, predicts the neuron's start from
-//              the chunk's published start and the expected counts
-//              (1 + budget each), and for the BATH_NC candidate starts around
-//              it finds c by a binary search of q[] (c - 1 sums below the
+//   warps 2, 3 convert groups of four rounds into the LUT index (uint32)(u*256)
+//              and the lapse factor -logf((float)(1-u)), and extend q[], the
+//              running sum over draws of one parity of the lapses in 2^-20
+//              units (q[n] = q[n-2] + round(lap[n] * 2^20), integers mod 2^32);
+//   warps 5-7, 9-11 (builders) tabulate the event counts of the chunk of 32
+//              neurons two chunks ahead of the walk.  The number of events c
+//              of a neuron is the first c at which nextBath + sum of c lapses
+//              * invNuExt reaches t+1; it depends on where in the stream the
+//              neuron starts, which is known only once every earlier neuron
+//              of the rank is decided.  Each neuron's budget (t+1 -
+//              nextBath)/invNuExt becomes two integer bounds that enclose
+//              every rounding of the reference's sequential sum; its start is
+//              predicted from the latest known chunk start and the expected
+//              counts (1 + budget each); for the BATH_NC candidate starts
+//              around the prediction (a warp per neuron, two candidates per
+//              lane) a binary search of q[] finds c (c - 1 sums below the
 //              lower bound, the c-th at or above the upper one); a candidate
-//              the bounds do not decide is marked undecided;
-//   warp 0     walks the neurons: per neuron one table lookup at its actual
-//              start gives c, so the serial chain is a subtraction, a shared
-//              load and an addition.  An undecided entry, a start outside
-//              the window, or the maxExternCurrentCount cap falls back to the
-//              reference's sequential loop.
-//              Then the 32 lanes write a chunk's events in parallel, each
-//              replaying its neuron in the reference's exact arithmetic.
+//              the bounds do not decide is marked undecided.  The builders
+//              then compose the tables: for every candidate start of neuron
+//              2p the events of neurons 2p and 2p+1 together, then of 4k ..
+//              4k+3 together;
+//   warp 0     (walk) follows the chain: one lookup per four neurons, at the
+//              quad's actual start, gives the next quad's start.  A quad the
+//              tables do not decide goes neuron by neuron, and an undecided
+//              neuron (or one at the maxExternCurrentCount cap) runs the
+//              reference's sequential loop.  The lanes then recover every
+//              neuron's start and count from the pair and single tables in
+//              parallel and hand the chunk to
+//   warp 4     (emitter), whose lanes write the chunk's events, each
+//              replaying its neuron in the reference's exact arithmetic;
+//   warp 8     stays idle: warps go to the SM's four schedulers by index, so
+//              the walk shares its scheduler with the emitter only.
 // Rounds are published in order with a flag; every wait is bounded and
 // raises F_BATH_DRAWS when its limit is reached.
 #define BATH_THREADS 384       // 12 warps: roles in bath_kernel
@@ -744,28 +750,58 @@ __global__ void __launch_bounds__(DELIVER_THREADS) deliver_kernel(Dev d) {
 #define BATH_AHEAD 2           // chunks the count tables are built ahead of the consumer (the code below
                                // predicts from chunk c-2's start)
 #define BATH_TABS (BATH_AHEAD + 1)
+#define BATH_CG 4              // generator rounds a converter takes at once: 96 draws, 3 per lane
+#define BATH_TROW (BATH_NC + 4)  // bytes per neuron in a count table: BATH_NC candidates, then the sentinel
+
+static_assert(BATH_NC == 64, "a builder lane takes two candidate starts");
+static_assert(24 * BATH_CG == 96 && BATH_ROUNDS % BATH_CG == 0, "a converter group is 3 draws per lane");
+
+// q[] keeps the two parities apart: draws n, n+2, n+4, .. sit in consecutive
+// words, so the 32 lanes of a builder, each on its own candidate start two
+// draws from the next, read 32 different banks.
+__device__ __forceinline__ uint32_t bath_qi(unsigned long long n) {
+  return (((uint32_t)n & 1u) * (BATH_RING / 2)) | (((uint32_t)n & (BATH_RING - 1)) >> 1);
+}
 
 struct BathSmem {
   uint32_t lap[BATH_RING];          // raw draw until converted, then the lapse (float bits)
-  uint32_t q[BATH_RING];            // per-parity prefix of the lapses, 2^-20 units
+  uint32_t q[BATH_RING];            // per-parity prefix of the lapses, 2^-20 units, at bath_qi(n)
   uint8_t idx[BATH_RING];
-  uint8_t tab[BATH_TABS][BATH_NC + 1][32];  // chunk c % BATH_TABS: events of neuron L started at
-                                    // bp_base + 2o, 0xFF = undecided; row BATH_NC: 0xFF (outside the window)
-  uint32_t bp_base[BATH_TABS][32];  // position (low 32 bits) of candidate 0 of neuron L
-  uint32_t bp_misc[BATH_TABS][32];  // 0: no bath event this step
+  // count tables of chunk c in buffer c % BATH_TABS.  Neuron j: its events
+  // when it starts at bp_base[j] + 2o, 0xFF = undecided; entries BATH_NC..
+  // answer a start outside the window (0xFF; 0 for a neuron with no event
+  // this step, whose every entry is 0).  Pair p, quad k: the events of
+  // neurons 2p, 2p+1 (4k .. 4k+3) when 2p (4k) starts at bp_base[2p] + 2o.
+  uint8_t tab[BATH_TABS][32][BATH_TROW];
+  uint8_t tab2[BATH_TABS][16][BATH_TROW];
+  uint8_t tab4[BATH_TABS][8][BATH_TROW];
+  uint32_t bp_base[BATH_TABS][32];  // position (low 32 bits) of candidate 0 of neuron j
   uint32_t tab_cnt[BATH_TABS];      // builder-warp completions of the tables of this buffer
-  uint32_t c_start[32], c_cnt[32];  // the consumer's decisions for the chunk being emitted
-  unsigned long long chunk_start[BATH_TABS];  // exact start of chunk c (consumer, as it begins chunk c)
+  uint32_t bld_sync;                // builder-warp arrivals at the table stages
+  uint32_t c_start[32], c_cnt[32];  // the walk's record: quad starts, and neurons walked one by one
+  uint32_t e_start[2][32], e_cnt[2][32];  // chunk c, handed to the emitter in buffer c & 1
+  unsigned long long e_end[2];      // its end position
+  uint32_t e_out[2];                // its first event slot
+  uint32_t e_seq, emit_done;        // chunks handed over, chunks emitted
+  unsigned long long emit_pos;      // ring slots before this position may be reused
+  unsigned long long chunk_start[BATH_TABS];  // exact start of chunk c (walk, as it begins chunk c)
   uint32_t chunk_seq;               // chunks whose start is published
   uint32_t flag[BATH_ROUNDS];       // round r converted <=> flag[r % BATH_ROUNDS] == r + 1
   uint32_t hist[64];
-  unsigned long long pos;           // consumer position (draws)
+  unsigned long long pos;           // walk position (draws)
   unsigned long long raw_end;       // draws generated
   unsigned long long conv_base;     // first draw of round 0 of this launch
-  uint32_t next_round;              // next round a converter claims
-  uint32_t published;               // rounds 0 .. published-1 are converted
+  uint32_t next_round;              // next group of BATH_CG rounds a converter claims
+  uint32_t published;               // rounds 0 .. published-1 are converted (raised after their flags)
   uint32_t done, err;
 };
+
+// The table entry for a start dl draws after candidate 0: dl / 2 for an
+// even dl inside the window, else BATH_NC (an odd dl rotates into the top
+// bit).
+__device__ __forceinline__ uint32_t bath_row(uint32_t dl) {
+  return min(__funnelshift_r(dl, dl, 1), (uint32_t)BATH_NC);
+}
 
 // logf of the host C library on (0,1]: a one-bit-per-float filter, then a
 // binary search of the fix-up keys.
@@ -835,8 +871,9 @@ __device__ static inline unsigned long long bath_exact(BathSmem &s, double nbv, 
   const uint32_t M = BATH_RING - 1;
   c = 0;
   while (lim < pos + 2ull * mx + 4) {
-    if (vs.flag[rr % BATH_ROUNDS] == rr + 1) {
-      rr++;
+    const uint32_t pb = vs.published;
+    if (pb > rr) {
+      rr = pb;
       lim = s.conv_base + (unsigned long long)rr * 24;
       __threadfence_block();
     } else if (++spins > BATH_SPIN_LIMIT) {
@@ -855,8 +892,9 @@ __device__ static inline unsigned long long bath_exact(BathSmem &s, double nbv, 
   if (c >= mx && nbv < T1) {
     do {   // single draws past the cap (rare)
       while (lim <= pos) {
-        if (vs.flag[rr % BATH_ROUNDS] == rr + 1) {
-          rr++;
+        const uint32_t pb = vs.published;
+        if (pb > rr) {
+          rr = pb;
           lim = s.conv_base + (unsigned long long)rr * 24;
           __threadfence_block();
         } else if (++spins > BATH_SPIN_LIMIT) {
@@ -869,6 +907,27 @@ __device__ static inline unsigned long long bath_exact(BathSmem &s, double nbv, 
     } while (nbv < T1);
   }
   return pos;
+}
+
+// The builder warps' meeting between table stages: each warp arrives, then
+// waits (bounded) until all BATH_BUILDERS have arrived `stage` times.  False
+// when the block is stopping.  Lane 0 waits; the answer is the warp's.
+__device__ static inline bool bath_builders_meet(BathSmem &s, uint32_t stage, uint32_t lane) {
+  volatile BathSmem &vs = s;
+  __syncwarp();
+  __threadfence_block();
+  bool ok = true;
+  if (lane == 0) {
+    atomicAdd(&s.bld_sync, 1u);
+    uint32_t sp = 0;
+    while (vs.bld_sync < BATH_BUILDERS * stage) {
+      if (vs.done) { ok = false; break; }
+      if (++sp > BATH_SPIN_LIMIT) { vs.err = 1; vs.done = 1; ok = false; break; }
+    }
+  }
+  ok = __shfl_sync(0xffffffffu, ok, 0);
+  __threadfence_block();
+  return ok;
 }
 
 __device__ static inline int bath_builder_index(uint32_t warp) {
@@ -901,12 +960,13 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
     s.done = 0;
     s.err = 0;
     s.chunk_seq = 0;
-    for (int b = 0; b < BATH_TABS; b++) {
-      s.tab_cnt[b] = 0;
-      for (int l = 0; l < 32; l++) s.tab[b][BATH_NC][l] = 0xFF;
-    }
-    s.q[(p0 - 2) & M] = 0;   // the prefix starts at p0 in each launch
-    s.q[(p0 - 1) & M] = 0;
+    s.bld_sync = 0;
+    s.e_seq = 0;
+    s.emit_done = 0;
+    s.emit_pos = p0;
+    for (int b = 0; b < BATH_TABS; b++) s.tab_cnt[b] = 0;
+    s.q[bath_qi(p0 - 2)] = 0;   // the prefix starts at p0 in each launch
+    s.q[bath_qi(p0 - 1)] = 0;
   }
   __syncthreads();
   if (warp == 0) {   // prefix of the restored draws [p0, q0)
@@ -917,9 +977,9 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
         const uint32_t y = __shfl_up_sync(0xffffffffu, v, o);
         if (lane >= (uint32_t)o) v += y;
       }
-      v += s.q[(n0 - 2 + (lane & 1)) & M];
+      v += s.q[bath_qi(n0 - 2 + (lane & 1))];
       __syncwarp();
-      if (n < q0) s.q[n & M] = v;
+      if (n < q0) s.q[bath_qi(n)] = v;
       __syncwarp();
     }
   }
@@ -934,7 +994,7 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
     while (true) {
       const unsigned long long n0 = s.conv_base + (unsigned long long)r * 24;
       uint32_t spins = 0;
-      while (!vs.done && n0 + 24 > vs.pos + BATH_RING - 64) {
+      while (!vs.done && n0 + 24 > vs.emit_pos + BATH_RING - 64) {
         if (++spins > BATH_SPIN_LIMIT) { vs.err = 1; vs.done = 1; break; }
         __nanosleep(64);   // leave the issue slots to the consumer
       }
@@ -956,7 +1016,7 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
       r++;
     }
   } else if (bath_builder_index(warp) >= 0) {
-    // ---- count tables, one chunk ahead of the consumer
+    // ---- count tables, two chunks ahead of the walk
     const uint32_t bw = (uint32_t)bath_builder_index(warp);
     unsigned long long pred = p0;   // predicted start of chunk c
     uint32_t exp1 = 0, exp2 = 0;    // expected events of chunks c-1 and c-2
@@ -1020,17 +1080,19 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
       const unsigned long long base = pred + 2ull * (incl - ec) - BATH_NC;
       if (bw == 0) {
         s.bp_base[b][lane] = (uint32_t)base;
-        s.bp_misc[b][lane] = misc;
+        *reinterpret_cast<uint32_t *>(&s.tab[b][lane][BATH_NC]) = misc ? 0xFFFFFFFFu : 0u;
       }
       // the draws every candidate of the chunk reads are converted; never
-      // beyond what the generator may produce ahead of the consumer (at
-      // least floor_pos + BATH_RING - 64): candidates past that stay undecided
+      // beyond what the generator may produce ahead of the walk (once the
+      // emitter is done with the chunks before c-2, at least floor_pos +
+      // BATH_RING - 64): candidates past that stay undecided
       const unsigned long long reach = floor_pos + BATH_RING - 512;
       const unsigned long long need =
           min(__shfl_sync(0xffffffffu, base, 31) + 2ull * BATH_NC + BATH_WINDOW, reach);
       while (lim < need) {
-        if (vs.flag[rr % BATH_ROUNDS] == rr + 1) {
-          rr++;
+        const uint32_t pb = vs.published;
+        if (pb > rr) {
+          rr = pb;
           lim = s.conv_base + (unsigned long long)rr * 24;
           __threadfence_block();
         } else if (vs.done) {
@@ -1046,42 +1108,85 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
         }
       }
       if (fail) break;
-      if (lane < cn && misc) {
-        // this warp's candidates o = bw, bw + BATH_BUILDERS, ..; for a start
-        // P the count is m + 1, m the number of k < 32 whose sum of the
-        // k+1 lapses at P+1, P+3, .., P+1+2k is below lo (the sums grow with
-        // k), when the (m+1)-th sum reaches hi1.  Positions are taken modulo
-        // 2^32 (a step reads far fewer draws); four candidates' binary
-        // searches run in lockstep, each probe round four independent loads.
-        const uint32_t cap = misc & 0xFFu, b32 = (uint32_t)base, f32 = (uint32_t)floor_pos;
+      // stage 1, this warp's neurons j = bw, bw + BATH_BUILDERS, ..; for
+      // neuron j the lanes take the candidates o = lane and lane + 32.  For
+      // a start P the count is m + 1, m the number of k < 32 whose sum of
+      // the k+1 lapses at P+1, P+3, .., P+1+2k is below lo (the sums grow
+      // with k), when the (m+1)-th sum reaches hi1.  Positions are taken
+      // modulo 2^32 (a step reads far fewer draws); the two candidates'
+      // binary searches run in lockstep.
+      {
+        const uint32_t b32 = (uint32_t)base, f32 = (uint32_t)floor_pos;
         const uint32_t r32 = (uint32_t)reach - BATH_WINDOW;
-        for (uint32_t o0 = bw; o0 < BATH_NC; o0 += 4 * BATH_BUILDERS) {
-          uint32_t P[4], qb[4], m[4];
-          bool ok[4];
+        for (uint32_t j = bw; j < 32; j += BATH_BUILDERS) {
+          const uint32_t mj = __shfl_sync(0xffffffffu, misc, j);
+          const uint32_t loj = __shfl_sync(0xffffffffu, lo, j), hij = __shfl_sync(0xffffffffu, hi1, j);
+          const uint32_t bj = __shfl_sync(0xffffffffu, b32, j);
+          uint8_t *row = s.tab[b][j];
+          if (!mj) {   // no bath event this step (or past the rank's last neuron): 0 from any start
+            row[lane] = 0;
+            row[lane + 32] = 0;
+            continue;
+          }
+          const uint32_t cap = mj & 0xFFu;
+          uint32_t P[2], qb[2], m[2];
+          bool ok[2];
 #pragma unroll
-          for (int v = 0; v < 4; v++) {
-            const uint32_t o = o0 + v * BATH_BUILDERS;
-            P[v] = b32 + 2u * o;
-            ok[v] = o < BATH_NC && (int32_t)(P[v] - f32) >= 0 && (int32_t)(r32 - P[v]) >= 0;
-            qb[v] = s.q[(P[v] - 1) & M];
+          for (int v = 0; v < 2; v++) {
+            P[v] = bj + 2u * (lane + 32u * v);
+            ok[v] = (int32_t)(P[v] - f32) >= 0 && (int32_t)(r32 - P[v]) >= 0;
+            qb[v] = s.q[bath_qi(P[v] - 1)];
             m[v] = 0;
           }
 #pragma unroll
           for (uint32_t st = 16; st > 0; st >>= 1) {
-            uint32_t f[4];
+            uint32_t f[2];
 #pragma unroll
-            for (int v = 0; v < 4; v++) f[v] = s.q[(P[v] + 1 + 2 * (m[v] + st - 1)) & M];
+            for (int v = 0; v < 2; v++) f[v] = s.q[bath_qi(P[v] + 1 + 2 * (m[v] + st - 1))];
 #pragma unroll
-            for (int v = 0; v < 4; v++) m[v] += (f[v] - qb[v] < lo) ? st : 0u;
+            for (int v = 0; v < 2; v++) m[v] += (f[v] - qb[v] < loj) ? st : 0u;
           }
 #pragma unroll
-          for (int v = 0; v < 4; v++) {
-            const uint32_t F = s.q[(P[v] + 1 + 2 * m[v]) & M] - qb[v];
-            const uint32_t mm = (m[v] == 31 && F < lo) ? 32u : m[v];
-            const uint32_t o = o0 + v * BATH_BUILDERS;
-            if (o < BATH_NC) s.tab[b][o][lane] = (ok[v] && mm < cap && F >= hi1) ? (uint8_t)(mm + 1) : (uint8_t)0xFF;
+          for (int v = 0; v < 2; v++) {
+            const uint32_t F = s.q[bath_qi(P[v] + 1 + 2 * m[v])] - qb[v];
+            const uint32_t mm = (m[v] == 31 && F < loj) ? 32u : m[v];
+            row[lane + 32 * v] = (ok[v] && mm < cap && F >= hij) ? (uint8_t)(mm + 1) : (uint8_t)0xFF;
           }
         }
+      }
+      // the composed tables' answers outside the window: 0 when none of
+      // their neurons has an event, else undecided
+      if (bw == 0) {
+        const uint32_t m2 = __shfl_sync(0xffffffffu, misc, (2 * lane) & 31) |
+                            __shfl_sync(0xffffffffu, misc, (2 * lane + 1) & 31);
+        const uint32_t m4 = __shfl_sync(0xffffffffu, m2, (2 * lane) & 31) |
+                            __shfl_sync(0xffffffffu, m2, (2 * lane + 1) & 31);
+        if (lane < 16) *reinterpret_cast<uint32_t *>(&s.tab2[b][lane][BATH_NC]) = m2 ? 0xFFFFFFFFu : 0u;
+        if (lane < 8) *reinterpret_cast<uint32_t *>(&s.tab4[b][lane][BATH_NC]) = m4 ? 0xFFFFFFFFu : 0u;
+      }
+      if (!bath_builders_meet(s, 2 * c + 1, lane)) { fail = true; break; }
+      // stage 2: pairs, from each candidate start of neuron 2p through 2p+1
+      for (uint32_t e = bw * 32 + lane; e < 16 * BATH_NC; e += 32 * BATH_BUILDERS) {
+        const uint32_t pp = e / BATH_NC, o = e % BATH_NC, a = 2 * pp;
+        const uint32_t ca = s.tab[b][a][o];
+        uint32_t v = 0xFFu;
+        if (ca != 0xFFu) {
+          const uint32_t cb = s.tab[b][a + 1][bath_row(s.bp_base[b][a] + 2 * (o + ca) - s.bp_base[b][a + 1])];
+          if (cb != 0xFFu) v = ca + cb;
+        }
+        s.tab2[b][pp][o] = (uint8_t)v;
+      }
+      if (!bath_builders_meet(s, 2 * c + 2, lane)) { fail = true; break; }
+      // stage 3: quads, from each candidate start of neuron 4k through its two pairs
+      for (uint32_t e = bw * 32 + lane; e < 8 * BATH_NC; e += 32 * BATH_BUILDERS) {
+        const uint32_t k = e / BATH_NC, o = e % BATH_NC, a = 4 * k;
+        const uint32_t va = s.tab2[b][2 * k][o];
+        uint32_t v = 0xFFu;
+        if (va != 0xFFu) {
+          const uint32_t vb = s.tab2[b][2 * k + 1][bath_row(s.bp_base[b][a] + 2 * (o + va) - s.bp_base[b][a + 2])];
+          if (vb != 0xFFu) v = va + vb;   // at most 4 x 32
+        }
+        s.tab4[b][k][o] = (uint8_t)v;
       }
       __syncwarp();
       __threadfence_block();
@@ -1089,62 +1194,76 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
       if (c0 + 32 < locN) prepare(c0 + 32);
     }
   } else if (warp == 2 || warp == 3) {
-    // ---- converters: rounds are claimed in order and published in order
+    // ---- converters: groups of BATH_CG rounds (3 draws per lane) are
+    // claimed in order and published in order
     while (true) {
-      uint32_t r = 0;
-      if (lane == 0) r = atomicAdd(&s.next_round, 1u);
-      r = __shfl_sync(0xffffffffu, r, 0);
-      const unsigned long long n0 = s.conv_base + (unsigned long long)r * 24;
+      uint32_t g = 0;
+      if (lane == 0) g = atomicAdd(&s.next_round, 1u);
+      g = __shfl_sync(0xffffffffu, g, 0);
+      const uint32_t r0 = g * BATH_CG;
+      const unsigned long long n0 = s.conv_base + (unsigned long long)r0 * 24;
       uint32_t spins = 0;
       bool quit = false;
       while (true) {
-        if (vs.raw_end >= n0 + 24) break;
+        if (vs.raw_end >= n0 + 24 * BATH_CG) break;
         if (vs.done) { quit = true; break; }
         if (++spins > BATH_SPIN_LIMIT) { vs.err = 1; vs.done = 1; quit = true; break; }
         __nanosleep(64);
       }
       if (quit) break;
       __threadfence_block();
-      uint8_t ix = 0;
-      float lp = 0.0f;
-      if (lane < 24) lp = bath_lapse(d, vs.lap[(n0 + lane) & M], ix);
-      uint32_t v = (lane < 24) ? lap_fixed(lp) : 0u;
-      for (int o = 2; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, v, o);
-        if (lane >= (uint32_t)o) v += y;
+      uint8_t ix[3];
+      float lp[3];
+      uint32_t v[3];
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        lp[i] = bath_lapse(d, vs.lap[(n0 + lane + 32 * i) & M], ix[i]);
+        v[i] = lap_fixed(lp[i]);
       }
-      // the previous round's prefix is final once its flag is set
-      if (r > 0) {
+      // per-parity prefix over the 96 draws: within each 32, then the
+      // totals of the earlier 32s (lanes 30, 31) carried
+      for (int o = 2; o < 32; o <<= 1) {
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+          const uint32_t y = __shfl_up_sync(0xffffffffu, v[i], o);
+          if (lane >= (uint32_t)o) v[i] += y;
+        }
+      }
+      const uint32_t c0 = __shfl_sync(0xffffffffu, v[0], 30 + (lane & 1));
+      const uint32_t c1 = __shfl_sync(0xffffffffu, v[1], 30 + (lane & 1));
+      v[1] += c0;
+      v[2] += c0 + c1;
+      // the previous group's prefix is final once its last flag is set
+      if (r0 > 0) {
         spins = 0;
         while (true) {
-          if (vs.flag[(r - 1) % BATH_ROUNDS] == r) break;
+          if (vs.flag[(r0 - 1) % BATH_ROUNDS] == r0) break;
           if (vs.done) { quit = true; break; }
           if (++spins > BATH_SPIN_LIMIT) { vs.err = 1; vs.done = 1; quit = true; break; }
           __nanosleep(32);
         }
-        if (quit) break;   // nothing of this round was written
+        if (quit) break;   // nothing of this group was written
         __threadfence_block();
       }
-      v += vs.q[(n0 - 2 + (lane & 1)) & M];
-      if (lane < 24) {
-        const uint32_t k = (uint32_t)(n0 + lane) & M;
-        s.lap[k] = __float_as_uint(lp);
-        s.idx[k] = ix;
-        s.q[k] = v;
+      const uint32_t qb = vs.q[bath_qi(n0 - 2 + (lane & 1))];
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        const unsigned long long n = n0 + lane + 32 * i;
+        s.lap[n & M] = __float_as_uint(lp[i]);
+        s.idx[n & M] = ix[i];
+        s.q[bath_qi(n)] = v[i] + qb;
       }
       __syncwarp();
       __threadfence_block();
-      if (lane == 0) {
-        vs.flag[r % BATH_ROUNDS] = r + 1;
-        vs.published = r + 1;
-      }
+      if (lane < BATH_CG) vs.flag[(r0 + lane) % BATH_ROUNDS] = r0 + lane + 1;
+      if (lane == 0) atomicMax(&s.published, r0 + BATH_CG);   // groups finish in order, their stores need not
     }
   } else if (warp == 0) {
-    // ---- consumer (warp 0)
+    // ---- walk (warp 0)
     unsigned long long pos = s.pos;
     unsigned long long lim = s.raw_end;   // converted draws available (prefix)
-    uint32_t rr = 0;                      // next round to check
-    uint32_t out = 0;
+    uint32_t rr = 0;                      // rounds known converted
+    uint32_t out = 0, spins = 0;
     bool fail = false;
     double nx_nb = 0, nx_inv = 0;
     uint32_t nx_mx = 0;
@@ -1154,10 +1273,10 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
       nx_mx = d.max_ext[i0 + lane];
     }
     for (uint32_t c0 = 0, ck = 0; c0 < locN && !fail; c0 += 32, ck++) {
-      const uint32_t cn = min(32u, locN - c0), tb = ck % BATH_TABS;
+      const uint32_t cn = min(32u, locN - c0), tb = ck % BATH_TABS, eb = ck & 1u;
       const double my_nb = nx_nb, my_inv = nx_inv;
       const uint32_t my_mx = nx_mx;
-      // this chunk's count table, then its start for the builders
+      // this chunk's count tables, then its start for the builders
       {
         uint32_t sp = 0;
         while (vs.tab_cnt[tb] < BATH_BUILDERS * (ck / BATH_TABS + 1)) {
@@ -1177,73 +1296,146 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
         nx_inv = d.inv_nu[i0 + c0 + 32 + lane];
         nx_mx = d.max_ext[i0 + c0 + 32 + lane];
       }
-      // the chunk's draws are converted (at most 2 * BATH_FAST_LANES per
-      // neuron through the table; a fall-back waits again for itself)
+      // the serial chain: one lookup per quad at its actual start; a run
+      // has no branch on the chain (an out-of-window start reads the
+      // sentinel); the first undecided quad is walked neuron by neuron
+      // below and the run goes on after it
       const unsigned long long base = pos;
-      uint32_t spins = 0;
-      while (lim < base + 64ull * BATH_FAST_LANES + BATH_WINDOW) {
-        if (vs.flag[rr % BATH_ROUNDS] == rr + 1) {
-          rr++;
-          lim = s.conv_base + (unsigned long long)rr * 24;
-          __threadfence_block();
-        } else if (++spins > BATH_SPIN_LIMIT) {
-          fail = true;
-          break;
-        }
-      }
-      if (fail) break;
-      // the serial chain: per neuron one table lookup at its actual start
-      const uint32_t *bb = s.bp_base[tb], *bm = s.bp_misc[tb];
-      const uint8_t *tab = &s.tab[tb][0][0];
-      uint32_t P = (uint32_t)base;
-      for (uint32_t j0 = 0; j0 < 32;) {
-        // a run with no branch on the chain: out-of-window starts read the
-        // sentinel row; the first undecided neuron is redone below
-        uint32_t bad = 32;
+      const uint32_t *bb = s.bp_base[tb];
+      const uint8_t *t1 = &s.tab[tb][0][0], *t2 = &s.tab2[tb][0][0], *t4 = &s.tab4[tb][0][0];
+      uint32_t P = (uint32_t)base, slow = 0;
+      for (uint32_t k0 = 0; k0 < 8;) {
+        uint32_t bad = 8;
 #pragma unroll 4
-        for (uint32_t j = j0; j < 32; j++) {
-          const uint32_t dl = P - bb[j];
-          const uint32_t row = ((dl & ~(uint32_t)(2 * BATH_NC - 2)) == 0) ? (dl >> 1) : (uint32_t)BATH_NC;
-          uint32_t cv = tab[row * 32 + j];
-          cv = bm[j] ? cv : 0u;
-          bad = (bad == 32 && cv == 0xFFu) ? j : bad;
+        for (uint32_t k = k0; k < 8; k++) {
+          const uint32_t v = t4[k * BATH_TROW + bath_row(P - bb[4 * k])];
+          bad = (bad == 8 && v == 0xFFu) ? k : bad;
+          if (lane == 0) s.c_start[4 * k] = P;
+          P += 2 * v;
+        }
+        if (bad == 8) break;
+        __syncwarp();
+        P = s.c_start[4 * bad];
+        for (uint32_t j = 4 * bad; j < 4 * bad + 4; j++) {
+          uint32_t cx = t1[j * BATH_TROW + bath_row(P - bb[j])];
+          uint32_t Pn = P + 2 * cx;
+          if (cx == 0xFFu) {
+            // the reference's loop from the actual start; the emitter
+            // first finishes the earlier chunks, so that the ring holds
+            // every draw the loop may read
+            uint32_t sp = 0;
+            while (vs.emit_done < ck) {
+              if (vs.err || ++sp > BATH_SPIN_LIMIT) { fail = true; break; }
+              __nanosleep(32);
+            }
+            if (fail) break;
+            const unsigned long long pj = base + (uint32_t)(P - (uint32_t)base);
+            const unsigned long long pe = bath_exact(s, __shfl_sync(0xffffffffu, my_nb, j),
+                                                     __shfl_sync(0xffffffffu, my_inv, j),
+                                                     __shfl_sync(0xffffffffu, my_mx, j), T1, pj, lim, rr, spins, fail, cx);
+            if (fail) break;
+            Pn = (uint32_t)pe;
+          }
           if (lane == 0) {
             s.c_start[j] = P;
-            s.c_cnt[j] = cv;
+            s.c_cnt[j] = cx;
           }
-          P += 2 * (cv & 0x3Fu);
+          P = Pn;
         }
-        if (bad == 32) break;
-        // the reference's loop for neuron `bad` from its actual start, then
-        // the run goes on after it
-        __syncwarp();
-        P = s.c_start[bad];
-        const unsigned long long pj = base + (uint32_t)(P - (uint32_t)base);
-        uint32_t cx = 0;
-        const unsigned long long pe = bath_exact(s, __shfl_sync(0xffffffffu, my_nb, bad),
-                                                 __shfl_sync(0xffffffffu, my_inv, bad),
-                                                 __shfl_sync(0xffffffffu, my_mx, bad), T1, pj, lim, rr, spins, fail, cx);
         if (fail) break;
-        if (lane == 0) s.c_cnt[bad] = cx;
-        P = (uint32_t)pe;
-        j0 = bad + 1;
+        slow |= 1u << bad;
+        k0 = bad + 1;
       }
       if (fail) break;
       __syncwarp();
-      const uint32_t my_cnt = (lane < cn) ? s.c_cnt[lane] : 0u;
-      const uint32_t my_start = s.c_start[lane];
+      // every neuron's start and events: from its quad's start through the
+      // pair and single tables (entries the quad's own entry was made of),
+      // or as the neuron-by-neuron walk recorded them
+      uint32_t my_start, my_cnt;
+      if ((slow >> (lane >> 2)) & 1u) {
+        my_start = s.c_start[lane];
+        my_cnt = s.c_cnt[lane];
+      } else {
+        uint32_t pq = s.c_start[lane & ~3u];
+        if (lane & 2u) pq += 2 * t2[((lane >> 1) & ~1u) * BATH_TROW + bath_row(pq - bb[lane & ~3u])];
+        if (lane & 1u) pq += 2 * t1[(lane & ~1u) * BATH_TROW + bath_row(pq - bb[lane & ~1u])];
+        my_start = pq;
+        my_cnt = t1[lane * BATH_TROW + bath_row(pq - bb[lane])];
+      }
+      if (lane >= cn) my_cnt = 0;
+      uint32_t tot = my_cnt;
+      for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
       pos = base + (uint32_t)(P - (uint32_t)base);
-      // parallel emission of the chunk's events
+      // hand the chunk to the emitter: buffer eb is free once chunk ck-2 is emitted
+      if (ck >= 2) {
+        uint32_t sp = 0;
+        while (vs.emit_done < ck - 1) {
+          if (vs.err || ++sp > BATH_SPIN_LIMIT) { fail = true; break; }
+          __nanosleep(32);
+        }
+        if (fail) break;
+      }
+      s.e_start[eb][lane] = my_start;
+      s.e_cnt[eb][lane] = my_cnt;
+      if (lane == 0) {
+        s.e_out[eb] = out;
+        s.e_end[eb] = pos;
+      }
+      out += tot;
+      __syncwarp();
+      __threadfence_block();
+      if (lane == 0) vs.e_seq = ck + 1;
+    }
+    if (lane == 0) {
+      if (fail) vs.err = 1;
+      vs.pos = pos;
+      __threadfence_block();
+      vs.done = 1;
+    }
+  } else if (warp == 4) {
+    // ---- emitter (warp 4): a chunk's events, each lane replaying its
+    // neuron in the reference's arithmetic
+    double nx_nb = 0, nx_inv = 0;
+    uint32_t nx_mx = 0;
+    if (lane < min(32u, locN)) {
+      nx_nb = d.nb_prev[i0 + lane];
+      nx_inv = d.inv_nu[i0 + lane];
+      nx_mx = d.max_ext[i0 + lane];
+    }
+    for (uint32_t c0 = 0, ck = 0; c0 < locN; c0 += 32, ck++) {
+      const uint32_t cn = min(32u, locN - c0), eb = ck & 1u;
+      const double my_nb = nx_nb, my_inv = nx_inv;
+      const uint32_t my_mx = nx_mx;
+      if (c0 + 32 < locN && lane < min(32u, locN - c0 - 32)) {
+        nx_nb = d.nb_prev[i0 + c0 + 32 + lane];
+        nx_inv = d.inv_nu[i0 + c0 + 32 + lane];
+        nx_mx = d.max_ext[i0 + c0 + 32 + lane];
+      }
+      bool quit = false;
+      uint32_t sp = 0;
+      while (vs.e_seq < ck + 1) {
+        if (vs.err) { quit = true; break; }
+        if (++sp > BATH_SPIN_LIMIT) { vs.err = 1; vs.done = 1; quit = true; break; }
+        __nanosleep(32);
+      }
+      if (__any_sync(0xffffffffu, quit)) break;
+      __threadfence_block();
+      const uint32_t my_start = s.e_start[eb][lane], my_cnt = s.e_cnt[eb][lane];
+      const uint32_t out = s.e_out[eb];
+      const unsigned long long end = s.e_end[eb];
+      if (__any_sync(0xffffffffu, lane < cn && my_cnt > my_mx)) {   // beyond the rank's event slots
+        if (lane == 0) { vs.err = 1; vs.done = 1; }
+        break;
+      }
       uint32_t incl = my_cnt;
       for (int o = 1; o < 32; o <<= 1) {
         const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= (uint32_t)o) incl += y;
       }
       const uint32_t my_off = out + incl - my_cnt;
-      out += __shfl_sync(0xffffffffu, incl, 31);
       if (lane < cn) {
         double v = my_nb;
-        unsigned long long p = my_start;
+        uint32_t p = my_start;
         double *bt = d.bath_time + ev_base + my_off;
         uint8_t *bl = d.bath_lut + ev_base + my_off;
         for (uint32_t c = 0; c < my_cnt; c++) {
@@ -1253,7 +1445,7 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
           p += 2;
         }
         if (my_cnt >= my_mx && my_cnt > 0 && v < T1) {
-          do {
+          do {   // single draws past the cap
             v += (double)__uint_as_float(s.lap[p & M]) * my_inv;
             p += 1;
           } while (v < T1);
@@ -1263,13 +1455,12 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
         d.bath_cnt[i0 + c0 + lane] = (uint16_t)my_cnt;
       }
       __syncwarp();
-      if (lane == 0) vs.pos = pos;   // ring slots before pos may now be reused
-    }
-    if (lane == 0) {
-      if (fail) vs.err = 1;
-      vs.pos = pos;
       __threadfence_block();
-      vs.done = 1;
+      if (lane == 0) {
+        vs.emit_pos = end;
+        __threadfence_block();
+        vs.emit_done = ck + 1;
+      }
     }
   }
   __syncthreads();
@@ -1299,28 +1490,41 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
   }
 }
 
-// LIFCADynamic, non-PerseoDyn branch (DPSNN_neuron_sim.c:664-824).
+// LIFCADynamic, non-PerseoDyn branch (DPSNN_neuron_sim.c:664-824): lifca_pre
+// below.
 struct NeuronRegs {
   double v, c, tr, te;
   int fired;
 };
-__device__ static inline void lifca(const NetConst *net, uint32_t s, NeuronRegs &n, double t, double I) {
-  double Tau = net->Tau[s], Theta = net->Theta[s], H = net->H[s], Tarp = net->Tarp[s];
-  double AlphaC = net->AlphaC[s], TauC = net->TauC[s], gC = net->gC[s];
-  double v = n.v, c = n.c, Tr = n.tr, Te = n.te;
-  double deltaT = t - Tr, TFLES = t - Te, rc, TrTe, dth, rmh;
+// The coefficients of one update: deltaT = t - Tr.  They depend on event
+// times only (Tr is the previous event's time), so the neuron run computes
+// them one event ahead, off the dependent chain of v and c.
+__device__ static inline void lifca_coeff(double Tau, double TauC, double deltaT, double &dth, double &rmh,
+                                          double &poly) {
+  dth = deltaT / 2;
+  rmh = dth / Tau;
+  const double rc = deltaT / TauC;
+  poly = 1 - rc + rc * rc / 2;
+}
+
+// LIFCADynamic with the coefficients of this event computed ahead; the branch
+// that leaves the refractory period moves deltaT, and recomputes them.
+__device__ static inline void lifca_pre(const NetConst *net, uint32_t s, NeuronRegs &n, double t, double I,
+                                        double dth, double rmh, double poly) {
+  const double Tau = net->Tau[s], Theta = net->Theta[s], H = net->H[s], Tarp = net->Tarp[s];
+  const double AlphaC = net->AlphaC[s], TauC = net->TauC[s], gC = net->gC[s];
+  double v = n.v, c = n.c, Te = n.te;
+  const double Tr = n.tr, TFLES = t - Te;
   if (TFLES > Tarp) {
-    TrTe = Tr - Te;
+    const double TrTe = Tr - Te;
     if (TrTe < Tarp) {
-      c *= exp_cr(-(deltaT - TFLES + Tarp) / TauC);
-      deltaT = TFLES - Tarp;
+      const double deltaT0 = t - Tr;
+      c *= exp_cr(-(deltaT0 - TFLES + Tarp) / TauC);
+      lifca_coeff(Tau, TauC, TFLES - Tarp, dth, rmh, poly);
     }
-    dth = deltaT / 2;
-    rmh = dth / Tau;
-    rc = deltaT / TauC;
     v = v - v * rmh - gC * c * dth;
     v = v - v * rmh - gC * c * dth;
-    c = c * (1 - rc + rc * rc / 2);
+    c = c * poly;
     v += I;
     if (v >= Theta) {
       v = H;
@@ -1329,8 +1533,7 @@ __device__ static inline void lifca(const NetConst *net, uint32_t s, NeuronRegs 
       n.fired = 1;
     }
   } else {
-    rc = deltaT / TauC;
-    c = c * (1 - rc + rc * rc / 2);
+    c = c * poly;
   }
   n.v = v;
   n.c = c;
@@ -1375,22 +1578,41 @@ __device__ static inline int run_neuron_ev(const Dev &d, uint32_t i, uint32_t t,
   const uint32_t boff = d.bath_off[i], bc = d.bath_cnt[i];
   const uint64_t bbase = d.bath_rank_base[i / net->locN] + boff;
   const double *lut = d.lut + (size_t)s * 256;
+  const double Tau = net->Tau[s], TauC = net->TauC[s];
   uint32_t a = 0, b = 0;
   double bt = (b < bc) ? d.bath_time[bbase] : 0.0;
-  while (a < ns || b < bc) {
-    double ct, I;
+  // the merge's next event (time, input)
+  auto next = [&](double &ct, double &I) -> bool {
     if (a < ns && (b >= bc || evs.time(a) <= bt)) {
       ct = evs.time(a);
       I = (double)evs.weight(a);
       a++;
-    } else {
+      return true;
+    }
+    if (b < bc) {
       ct = bt;
       I = lut[d.bath_lut[bbase + b]];
       b++;
       if (b < bc) bt = d.bath_time[bbase + b];
+      return true;
     }
+    return false;
+  };
+  double ct = 0, I = 0, dth = 0, rmh = 0, poly = 0;
+  bool have = next(ct, I);
+  if (have) lifca_coeff(Tau, TauC, ct - n.tr, dth, rmh, poly);
+  while (have) {
+    double ct1 = 0, I1 = 0, dth1 = 0, rmh1 = 0, poly1 = 0;
+    const bool have1 = next(ct1, I1);
+    if (have1) lifca_coeff(Tau, TauC, ct1 - ct, dth1, rmh1, poly1);   // after this event Tr = ct
     if (((ct - T0) >= 1.0) || ((ct - T0) < 0)) atomicOr(d.flags, F_TIME_WINDOW);
-    lifca(net, s, n, ct, I);
+    lifca_pre(net, s, n, ct, I, dth, rmh, poly);
+    ct = ct1;
+    I = I1;
+    dth = dth1;
+    rmh = rmh1;
+    poly = poly1;
+    have = have1;
   }
   d.v[i] = n.v;
   d.c[i] = n.c;
@@ -1480,12 +1702,12 @@ __global__ void __launch_bounds__(NEURON_BLOCK) neuron_kernel(Dev d) {
 
 // Heavy neurons, more than LOCAL_EVENTS synaptic events in one step.
 // heavy_sort_kernel: one warp per neuron with at most HEAVY_WARP_MAX events
-// loads its bucket into registers, computes the arrival times,
-// bitonic-sorts by (time, key) and writes the sorted events back into the
-// bucket; heavy_run_kernel then runs those neurons one thread each.  Neurons
-// with more events (including any beyond the bucket, in the overflow list)
-// are sorted and run by huge_kernel, one block each.
-#define HEAVY_WARP_MAX 256     // events a warp sorts in registers (8 per lane)
+// loads its bucket into registers, computes the arrival times, sorts by
+// (time, key) and writes the sorted events back into the bucket;
+// heavy_run_kernel then runs those neurons one thread each.  Neurons with
+// more events (including any beyond the bucket, in the overflow list) are
+// sorted and run by huge_kernel, one block each.
+#define HEAVY_WARP_MAX 256     // events a warp sorts (8 per lane)
 #define HEAVY_MAX 8192
 #define HEAVY_THREADS 256
 #define HEAVY_SMEM (HEAVY_MAX * 16)
@@ -1523,138 +1745,111 @@ __device__ static inline uint32_t warp_path_max(const NetConst *net) {
   return min(net->ev_cap / 2, (uint32_t)HEAVY_WARP_MAX);
 }
 
-// Bitonic sort of 32*E events held in registers, E per lane: element
-// e = lane*E + r sits in register r of its lane.  An element is (arrival
-// time as IEEE bits, key, weight): times are positive, so their bit
-// patterns order like the times, and equal times order by key, which is
-// unique per target.  Exchanges between positions closer than E stay in the
-// lane's registers; the 15 farther ones (for E = 8) are one shuffle per
-// 32-bit word.  Ascending order at the end.
-template <int E>
-__device__ static inline void cas_in_lane(uint64_t (&tb)[E], uint32_t (&ky)[E], uint32_t (&wv)[E], int r, int q,
-                                          bool up) {
-  const bool gt = (tb[r] > tb[q]) || (tb[r] == tb[q] && ky[r] > ky[q]);
-  if (gt == up) {
-    const uint64_t t0 = tb[r];
-    tb[r] = tb[q];
-    tb[q] = t0;
-    const uint32_t k0 = ky[r];
-    ky[r] = ky[q];
-    ky[q] = k0;
-    const uint32_t w0 = wv[r];
-    wv[r] = wv[q];
-    wv[q] = w0;
-  }
-}
+// A warp's sort of one heavy neuron's events: a bucket sort on the arrival
+// time.  Arrival times lie in [t, t+1); bucket (time - t) * 256 is monotone
+// in the time, so buckets order the events, and inside a bucket each event's
+// place is the number of the bucket's events before it in (time, key) order
+// (keys are unique per target).  Buckets are small unless many events share
+// one arrival time, as a cascade's do; then the count is quadratic in the
+// bucket's size, spread over the lanes.
+#define HS_BUCKETS 256
 
-// The in-lane stages j = J, J/2, .., 1 of one merge step k (k may be a
-// runtime value: the direction of a pair depends on bit k of its position).
-template <int E, int J>
-__device__ static inline void in_lane_stages(uint64_t (&tb)[E], uint32_t (&ky)[E], uint32_t (&wv)[E], uint32_t lane,
-                                             uint32_t k) {
-  if constexpr (J >= 1) {
-#pragma unroll
-    for (int r = 0; r < E; r++)
-      if (!(r & J)) cas_in_lane<E>(tb, ky, wv, r, r | J, ((lane * E + r) & k) == 0);
-    in_lane_stages<E, J / 2>(tb, ky, wv, lane, k);
-  }
-}
+struct HeavySortWarp {
+  uint32_t start[HS_BUCKETS + 1];   // counts, then the buckets' first positions
+  double tau[HEAVY_WARP_MAX];       // events staged by bucket for the counts
+  uint32_t key[HEAVY_WARP_MAX];
+};
 
-// Bitonic sort of 32*E events held in registers, E per lane: element
-// e = lane*E + r sits in register r of its lane.  An element is (arrival
-// time as IEEE bits, key, weight): times are positive, so their bit
-// patterns order like the times, and equal times order by key, which is
-// unique per target.  Exchanges between positions closer than E stay in the
-// lane's registers (unrolled, so that register indices are constants); the
-// farther ones are one shuffle per 32-bit word, in a loop (the network
-// fully unrolled does not fit the instruction cache).  Ascending order.
-template <int E>
-__device__ static inline void warp_sort_events(uint64_t (&tb)[E], uint32_t (&ky)[E], uint32_t (&wv)[E],
-                                               uint32_t lane) {
-  // merge steps k <= E: inside each lane's E registers
-#pragma unroll
-  for (int k = 2; k <= E; k <<= 1) {
-    if (k == 2) in_lane_stages<E, 1>(tb, ky, wv, lane, 2);
-    if (k == 4) in_lane_stages<E, 2>(tb, ky, wv, lane, 4);
-    if (k == 8) in_lane_stages<E, 4>(tb, ky, wv, lane, 8);
-  }
-  // merge steps k > E: exchanges across lanes down to distance E, then in-lane
-#pragma unroll 1
-  for (uint32_t k = 2 * E; k <= 32u * E; k <<= 1) {
-#pragma unroll 1
-    for (uint32_t j = k >> 1; j >= (uint32_t)E; j >>= 1) {
-      const uint32_t m = j / E;
-      const bool lower = (lane & m) == 0;
-#pragma unroll
-      for (int r = 0; r < E; r++) {
-        const bool up = ((lane * E + r) & k) == 0;
-        const uint32_t ylo = __shfl_xor_sync(0xffffffffu, (uint32_t)tb[r], m);
-        const uint32_t yhi = __shfl_xor_sync(0xffffffffu, (uint32_t)(tb[r] >> 32), m);
-        const uint32_t yk = __shfl_xor_sync(0xffffffffu, ky[r], m);
-        const uint32_t yw = __shfl_xor_sync(0xffffffffu, wv[r], m);
-        const uint64_t yt = ((uint64_t)yhi << 32) | ylo;
-        const bool x_lt_y = (tb[r] < yt) || (tb[r] == yt && ky[r] < yk);
-        // the lower position of an ascending pair keeps the smaller one
-        if ((lower == up) ? !x_lt_y : x_lt_y) {
-          tb[r] = yt;
-          ky[r] = yk;
-          wv[r] = yw;
-        }
-      }
-    }
-    in_lane_stages<E, E / 2>(tb, ky, wv, lane, k);
-  }
-}
-
-// One heavy neuron's n <= 32*E events: loaded with their arrival times,
-// sorted by (time, key) in registers, written back as sorted times into
-// the bucket's first half and weights into its second half.
+// One heavy neuron's n <= 32*E events (element e = lane + 32r in register r):
+// loaded with their arrival times, sorted by (time, key), written back as
+// sorted times into the bucket's first half and weights into its second half.
 template <int E>
 __device__ static inline void heavy_sort_one(const Dev &d, uint2 *ev, uint32_t n, uint32_t t, uint32_t D,
-                                             uint32_t N, uint32_t cap, uint32_t lane) {
-  uint64_t tb[E];
-  uint32_t ky[E], wv[E];
+                                             uint32_t N, uint32_t cap, uint32_t lane, HeavySortWarp &w) {
+  const double T0 = (double)t;
+  for (uint32_t b = lane; b <= HS_BUCKETS; b += 32) w.start[b] = 0;
   uint2 x[E];
 #pragma unroll
   for (int r = 0; r < E; r++) {
-    const uint32_t e = lane * E + r;
+    const uint32_t e = lane + 32u * r;
     if (e < n) x[r] = ev[e];
   }
+  __syncwarp();
+  double tau[E];
+  uint32_t bs[E];   // bucket << 16 | place among the bucket's events in arrival order
 #pragma unroll
   for (int r = 0; r < E; r++) {
-    const uint32_t e = lane * E + r;
+    const uint32_t e = lane + 32u * r;
     if (e < n) {
-      tb[r] = (uint64_t)__double_as_longlong(event_time(d, x[r].x, t, D, N));
-      ky[r] = x[r].x;
-      wv[r] = x[r].y;
-    } else {   // padding after every event: +infinity, largest key
-      tb[r] = 0x7FF0000000000000ull;
-      ky[r] = 0xFFFFFFFFu;
-      wv[r] = 0u;
+      tau[r] = event_time(d, x[r].x, t, D, N);
+      const uint32_t b = min((uint32_t)((tau[r] - T0) * (double)HS_BUCKETS), (uint32_t)HS_BUCKETS - 1);
+      bs[r] = (b << 16) | atomicAdd(&w.start[b], 1u);
     }
   }
-  warp_sort_events<E>(tb, ky, wv, lane);
-  __syncwarp();   // every lane has read its events before the bucket is overwritten
+  __syncwarp();
+  // exclusive prefix of the counts, 8 consecutive buckets per lane
+  {
+    uint32_t c[HS_BUCKETS / 32], tot = 0;
+#pragma unroll
+    for (int i = 0; i < HS_BUCKETS / 32; i++) {
+      c[i] = w.start[lane * (HS_BUCKETS / 32) + i];
+      const uint32_t v = c[i];
+      c[i] = tot;
+      tot += v;
+    }
+    uint32_t incl = tot;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= (uint32_t)o) incl += y;
+    }
+#pragma unroll
+    for (int i = 0; i < HS_BUCKETS / 32; i++) w.start[lane * (HS_BUCKETS / 32) + i] = incl - tot + c[i];
+    if (lane == 31) w.start[HS_BUCKETS] = incl;
+  }
+  __syncwarp();
+  // staged by bucket; bs becomes bucket << 16 | staged position
+#pragma unroll
+  for (int r = 0; r < E; r++) {
+    const uint32_t e = lane + 32u * r;
+    if (e < n) {
+      const uint32_t b = bs[r] >> 16, p = w.start[b] + (bs[r] & 0xFFFFu);
+      w.tau[p] = tau[r];
+      w.key[p] = x[r].x;
+      bs[r] = (b << 16) | p;
+    }
+  }
+  __syncwarp();
   double *st = reinterpret_cast<double *>(ev);
   float *sv = reinterpret_cast<float *>(ev + cap / 2);
 #pragma unroll
   for (int r = 0; r < E; r++) {
-    const uint32_t e = lane * E + r;
+    const uint32_t e = lane + 32u * r;
     if (e < n) {
-      st[e] = __longlong_as_double((long long)tb[r]);
-      sv[e] = __uint_as_float(wv[r]);
+      const uint32_t b = bs[r] >> 16, p = bs[r] & 0xFFFFu;
+      const uint32_t b0 = w.start[b], b1 = w.start[b + 1], k = w.key[p];
+      const double tm = w.tau[p];
+      uint32_t rank = 0;
+      for (uint32_t j = b0; j < b1; j++) {
+        const double tj = w.tau[j];
+        rank += (tj < tm) || (tj == tm && w.key[j] < k);
+      }
+      st[b0 + rank] = tm;
+      sv[b0 + rank] = __uint_as_float(x[r].y);
     }
   }
+  __syncwarp();   // the warp's next neuron reuses the staging arrays
 }
 
 #define HEAVY_SORT_THREADS 256
 
-// A warp per neuron of the warp path (LOCAL_EVENTS < n <= HEAVY_WARP_MAX):
-// registers only, no shared memory.
+// A warp per neuron of the warp path (LOCAL_EVENTS < n <= HEAVY_WARP_MAX),
+// each warp with its own bucket-sort arrays in shared memory.
 __global__ void __launch_bounds__(HEAVY_SORT_THREADS, 2) heavy_sort_kernel(Dev d) {
+  __shared__ HeavySortWarp s_ws[HEAVY_SORT_THREADS / 32];
   const NetConst *net = d.net;
   const uint32_t t = *d.t, N = net->N, D = net->D, cap = net->ev_cap, wmax = warp_path_max(net);
   const uint32_t lane = threadIdx.x & 31;
+  HeavySortWarp &ws = s_ws[threadIdx.x >> 5];
   const uint32_t nh = min(d.heavy_cnt[0], N);
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t hh = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; hh < nh; hh += nwarps) {
@@ -1662,13 +1857,13 @@ __global__ void __launch_bounds__(HEAVY_SORT_THREADS, 2) heavy_sort_kernel(Dev d
     if (n > wmax) continue;   // not listed here
     uint2 *ev = d.ev + (size_t)i * cap;
     if (n <= 32)
-      heavy_sort_one<1>(d, ev, n, t, D, N, cap, lane);
+      heavy_sort_one<1>(d, ev, n, t, D, N, cap, lane, ws);
     else if (n <= 64)
-      heavy_sort_one<2>(d, ev, n, t, D, N, cap, lane);
+      heavy_sort_one<2>(d, ev, n, t, D, N, cap, lane, ws);
     else if (n <= 128)
-      heavy_sort_one<4>(d, ev, n, t, D, N, cap, lane);
+      heavy_sort_one<4>(d, ev, n, t, D, N, cap, lane, ws);
     else
-      heavy_sort_one<8>(d, ev, n, t, D, N, cap, lane);
+      heavy_sort_one<8>(d, ev, n, t, D, N, cap, lane, ws);
   }
 }
 
@@ -1676,7 +1871,7 @@ __global__ void __launch_bounds__(HEAVY_SORT_THREADS, 2) heavy_sort_kernel(Dev d
 // (arrival times, then weights); same merge and arithmetic as run_neuron.
 __global__ void heavy_run_kernel(Dev d) {
   const NetConst *net = d.net;
-  const uint32_t t = *d.t, N = net->N, D = net->D, cap = net->ev_cap, wmax = warp_path_max(net);
+  const uint32_t t = *d.t, N = net->N, cap = net->ev_cap, wmax = warp_path_max(net);
   const uint32_t nh = min(d.heavy_cnt[0], N);
   for (uint32_t hh = blockIdx.x * blockDim.x + threadIdx.x; hh < nh; hh += gridDim.x * blockDim.x) {
     const uint32_t i = d.heavy_list[hh], ns = d.heavy_list[N + hh];
@@ -1684,48 +1879,7 @@ __global__ void heavy_run_kernel(Dev d) {
     const uint2 *ev = d.ev + (size_t)i * cap;
     const double *st = reinterpret_cast<const double *>(ev);
     const float *sv = reinterpret_cast<const float *>(ev + cap / 2);
-    const uint32_t s = d.sub[i];
-    NeuronRegs n;
-    n.v = d.v[i];
-    n.c = d.c[i];
-    n.tr = d.tr[i];
-    n.te = d.te[i];
-    n.fired = 0;
-    const double T0 = (double)t;
-    const uint32_t bc = d.bath_cnt[i];
-    const uint64_t bbase = d.bath_rank_base[i / net->locN] + d.bath_off[i];
-    const double *lut = d.lut + (size_t)s * 256;
-    uint32_t a = 0, b = 0;
-    double bt = (b < bc) ? d.bath_time[bbase] : 0.0;
-    double at = st[0];
-    float aw = sv[0];
-    while (a < ns || b < bc) {
-      double ct, I;
-      if (a < ns && (b >= bc || at <= bt)) {
-        ct = at;
-        I = (double)aw;
-        a++;
-        if (a < ns) {
-          at = st[a];
-          aw = sv[a];
-        }
-      } else {
-        ct = bt;
-        I = lut[d.bath_lut[bbase + b]];
-        b++;
-        if (b < bc) bt = d.bath_time[bbase + b];
-      }
-      if (((ct - T0) >= 1.0) || ((ct - T0) < 0)) atomicOr(d.flags, F_TIME_WINDOW);
-      lifca(net, s, n, ct, I);
-    }
-    d.v[i] = n.v;
-    d.c[i] = n.c;
-    d.tr[i] = n.tr;
-    d.te[i] = n.te;
-    if (n.fired) {
-      d.fired[i] = 1;
-      atomicAdd(&d.block_fired[i / NEURON_BLOCK], 1u);
-    }
+    if (run_neuron_ev(d, i, t, EvArrays{st, sv}, ns)) atomicAdd(&d.block_fired[i / NEURON_BLOCK], 1u);
   }
 }
 
@@ -1935,6 +2089,7 @@ struct dpsnn_engine {
   std::vector<void *> temps;       // build scratch, released when the build ends
   uint64_t bytes = 0;              // device memory held (allocs)
   uint32_t grid_neuron = 0, grid_deliver = 0, grid_heavy = 0, grid_heavy_run = 0, grid_huge = 0;
+  int sms = 148;                   // the device's SMs (default grids)
   int timing = 0;
   bool capturing = false;          // steps are being recorded into a graph
   struct TimedLaunch { int family; cudaEvent_t a, b; cudaStream_t st; };
@@ -2462,6 +2617,7 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
   if (rc) return rc;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
+  e->sms = sms;
   e->grid_deliver = (uint32_t)sms * 8;
   e->grid_heavy = (uint32_t)sms * 8;
   e->grid_heavy_run = (uint32_t)sms * 16;
@@ -2848,6 +3004,18 @@ extern "C" int dpsnn_graph_run(dpsnn_graph *g) {
     e->t_host += g->nsteps;
   }
   g->engines[0]->launches += g->launches_per_run;   // counted on the first engine
+  return 0;
+}
+
+extern "C" int dpsnn_set_launch_shape(dpsnn_engine *e, uint32_t deliver_blocks, uint32_t heavy_sort_blocks,
+                                      uint32_t heavy_run_blocks) {
+  if (!e) return dpsnn_fail(DPSNN_E_PARAM, "null engine");
+  const uint32_t lim = 1u << 20;
+  if (deliver_blocks > lim || heavy_sort_blocks > lim || heavy_run_blocks > lim)
+    return dpsnn_fail(DPSNN_E_PARAM, "a grid of more than %u blocks", lim);
+  e->grid_deliver = deliver_blocks ? deliver_blocks : (uint32_t)e->sms * 8;
+  e->grid_heavy = heavy_sort_blocks ? heavy_sort_blocks : (uint32_t)e->sms * 8;
+  e->grid_heavy_run = heavy_run_blocks ? heavy_run_blocks : (uint32_t)e->sms * 16;
   return 0;
 }
 

@@ -57,7 +57,8 @@ EXPORTS = [
     "dpsnn_bath_params", "dpsnn_set_timing", "dpsnn_kernel_times", "dpsnn_kernel_launches", "dpsnn_cuda_stream",
     "dpsnn_rank_spikes_noalloc", "dpsnn_enable_ltp_probe", "dpsnn_ltp_probe",
     "dpsnn_enable_stdp_events", "dpsnn_stdp_events", "dpsnn_step_many", "dpsnn_last_error",
-    "dpsnn_spikes_range", "dpsnn_device_bytes",
+    "dpsnn_spikes_range", "dpsnn_device_bytes", "dpsnn_graph_create", "dpsnn_graph_run", "dpsnn_graph_destroy",
+    "dpsnn_set_launch_shape",
 ]
 NOALLOC_MAX_SPIKES = 32768   # DPSNN_NOALLOC_MAX_SPIKES
 TIMING_SLOTS = 8             # DPSNN_TIMING_SLOTS
@@ -112,6 +113,11 @@ def load_library(path: str = LIB_PATH):
     lib.dpsnn_spikes_range.argtypes = [P, C.c_uint32, C.c_uint32, P, P, C.c_uint64, P]
     lib.dpsnn_device_bytes.argtypes = [P]
     lib.dpsnn_device_bytes.restype = C.c_uint64
+    lib.dpsnn_graph_create.argtypes = [P, C.c_uint32, C.c_uint32, C.POINTER(P)]
+    lib.dpsnn_graph_run.argtypes = [P]
+    lib.dpsnn_graph_destroy.argtypes = [P]
+    lib.dpsnn_graph_destroy.restype = None
+    lib.dpsnn_set_launch_shape.argtypes = [P, C.c_uint32, C.c_uint32, C.c_uint32]
     lib.dpsnn_last_error.restype = C.c_char_p
     _LIB = lib
     return lib
@@ -252,6 +258,13 @@ class Engine:
         """Device memory the engine holds."""
         return self._L.dpsnn_device_bytes(self._h)
 
+    def set_launch_shape(self, deliver_blocks: int = 0, heavy_sort_blocks: int = 0, heavy_run_blocks: int = 0):
+        """Grid sizes of the delivery, warp-sort and heavy-run kernels (0 =
+        the defaults, sized for a network that fills the GPU); results do
+        not depend on them."""
+        self._check(self._L.dpsnn_set_launch_shape(self._h, deliver_blocks, heavy_sort_blocks, heavy_run_blocks),
+                    "dpsnn_set_launch_shape")
+
     def rank_spikes_noalloc(self, t_ms: int, rank: int):
         """Spikes of one emulated rank at step t_ms, gathered without any
         device allocation (dpsnn_rank_spikes_noalloc)."""
@@ -356,3 +369,37 @@ def step_many(engines, n: int):
     rc = lib.dpsnn_step_many(arr, len(engines), n)
     if rc != 0:
         raise EngineError(f"dpsnn_step_many failed ({rc}): {lib.dpsnn_last_error().decode()}")
+
+
+class Graph:
+    """``nsteps`` steps (a multiple of 80) of every engine, in
+    :func:`step_many`'s order, recorded once into a CUDA graph
+    (dpsnn_graph_create); :meth:`run` advances every engine by ``nsteps``
+    steps in one launch.  The engines must have run their first step."""
+
+    def __init__(self, engines, nsteps: int):
+        self._L = load_library()
+        self.engines = list(engines)
+        self.nsteps = nsteps
+        arr = (C.c_void_p * len(self.engines))(*[e._h for e in self.engines])
+        g = C.c_void_p()
+        rc = self._L.dpsnn_graph_create(arr, len(self.engines), nsteps, C.byref(g))
+        if rc != 0:
+            raise EngineError(f"dpsnn_graph_create failed ({rc}): {self._L.dpsnn_last_error().decode()}")
+        self._g = g
+
+    def run(self):
+        rc = self._L.dpsnn_graph_run(self._g)
+        if rc != 0:
+            raise EngineError(f"dpsnn_graph_run failed ({rc}): {self._L.dpsnn_last_error().decode()}")
+
+    def close(self):
+        if self._g:
+            self._L.dpsnn_graph_destroy(self._g)
+            self._g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

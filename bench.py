@@ -15,9 +15,9 @@ e2e    = the same metric through the C ABI as a drop-in caller uses it: one
          dpsnn_step per ms and the step's spike list read back to host memory
          (the raster), timed on the host; no per-step input goes to the device.
 --batch J runs the batched sweep instead: J independent networks of 1x1-4x4
-modules, --batch-ms biological ms of each, stepped together (dpsnn_step_many)
-and, on freshly built engines, one after another (dpsnn_step), printing one
-JSON line with both aggregate rates.
+modules, --batch-ms biological ms of each, one after another (dpsnn_step),
+together (dpsnn_step_many) and together in autotuned CUDA graphs of 80 steps,
+printing one JSON line with the three aggregate rates.
 The reference arm (--impl reference) runs the reference built from its
 sources on the same network and steps as the engine's timed region, as 192
 MPI processes (a forked shared-memory MPI subset, oracle/mpi_shm) on the
@@ -298,78 +298,84 @@ def run_reference(args, world, rank):
     }))
 
 
-def batch_jobs(n_jobs: int, ms: int):
-    """The batched sweep: independent networks of 1x1 to 4x4 modules (uniform),
-    each with its own seed, external Poisson rate (1-5 kHz: NuExt 1-5 Hz over
-    CExt 1000) and calcium adaptation increment (0-2x the baseline 1.0)."""
-    import numpy as np
-    nc = importlib.import_module("201812realtimecortsim_b200.netconfig")
-    rng = np.random.default_rng(2024)
-    jobs = []
-    for i in range(n_jobs):
-        g = int(rng.integers(1, 5))
-        nu, alpha = float(rng.uniform(1.0, 5.0)), float(rng.uniform(0.0, 2.0))
-        kw = {"p1": 0.0376} if g <= 2 else {}
-        jobs.append(nc.cortical_grid(g, g, total_ms=ms + 10, seed=1 + i, nu_ext_hz=nu, alpha_c=alpha, **kw))
-    return jobs
-
-
 def run_batch(args):
-    """One JSON line for the batched form: the jobs run together through
-    dpsnn_step_many against the same jobs issued one at a time with
-    dpsnn_step, each arm on freshly built engines, host wall time between
-    device synchronisations (the arms span many streams)."""
+    """One JSON line for the batched form: the same jobs (batch.sweep_configs)
+    on freshly built engines in three arms, each timed over steps 1..K after
+    an untimed first step (K = --batch-ms rounded up to a multiple of 80):
+      sequential -- one job after another, dpsnn_step;
+      step_many  -- all jobs together, dpsnn_step_many (one step of every
+                    job at a time, their kernels overlapping);
+      graph      -- all jobs together in CUDA graphs of 80 steps, with the
+                    launch shapes the autotuner picked (tuned untimed on the
+                    step_many arm's engines after their timed region).
+    Host wall time between device synchronisations (the arms span many
+    streams); each arm's per-job event counts must be identical."""
     import torch
     E = importlib.import_module("201812realtimecortsim_b200.engine")
-    jobs = batch_jobs(args.batch, args.batch_ms)
-    res = {}
-    build_s = {}
-    for arm in ("sequential", "batched"):
+    B = importlib.import_module("201812realtimecortsim_b200.batch")
+    K = -(-max(args.batch_ms, 1) // B.GRAPH_STEPS) * B.GRAPH_STEPS
+    tune_steps = len(B.CANDIDATES) * 2 * B.GRAPH_STEPS
+    jobs = B.sweep_configs(args.batch, total_ms=K + tune_steps + 10)
+    sync = torch.cuda.synchronize
+    res, build_s, extra = {}, {}, {}
+    best_rule = None
+    for arm in ("sequential", "step_many", "graph"):
         tb0 = time.perf_counter()
-
-        def build(c):
-            # a build is seconds of serial per-module ran3 streams on a few GPU
-            # threads whatever the network's size: builds from several host
-            # threads overlap (the engine call releases the GIL)
-            tj = time.perf_counter()
-            e = E.Engine(c, device=0)
-            print(f"[batch] {arm}: built {c.cfx}x{c.cfy} ({c.glob_n} neurons) in "
-                  f"{time.perf_counter() - tj:.3f} s", file=sys.stderr, flush=True)
-            return e
-
-        with concurrent.futures.ThreadPoolExecutor(max_workers=min(32, len(jobs))) as pool:
-            engines = list(pool.map(build, jobs))
-        torch.cuda.synchronize()
+        engines = B.build_all(jobs, threads=16)
+        sync()
+        build_s[arm] = time.perf_counter() - tb0
+        if arm == "graph":
+            for e, c in zip(engines, jobs):
+                e.set_launch_shape(*best_rule(e, c))
+        E.step_many(engines, 1)
+        for e in engines:
+            e.sync()
+        ev0 = [e.events_delivered() for e in engines]
+        runner = None
+        if arm == "graph":
+            tg = time.perf_counter()
+            runner = B.BatchRunner(engines)
+            extra["graph_record_s"] = time.perf_counter() - tg
+        sync()
         t0 = time.perf_counter()
-        build_s[arm] = t0 - tb0
         if arm == "sequential":
-            for c, e in zip(jobs, engines):
-                tj = time.perf_counter()
-                e.step(args.batch_ms)
-                e.sync()
-                print(f"[batch] sequential: {c.cfx}x{c.cfy} stepped {args.batch_ms} ms in "
-                      f"{time.perf_counter() - tj:.3f} s", file=sys.stderr, flush=True)
-        else:
-            E.step_many(engines, args.batch_ms)
             for e in engines:
+                e.step(K)
                 e.sync()
-        torch.cuda.synchronize()
+        elif arm == "step_many":
+            E.step_many(engines, K)
+        else:
+            runner.run(K)
+        for e in engines:
+            e.sync()
+        sync()
         dt = time.perf_counter() - t0
-        ev = [e.events_delivered() for e in engines]
+        ev = [e.events_delivered() - a for e, a in zip(engines, ev0)]
         res[arm] = (dt, ev)
+        print(f"[batch] {arm}: {K} steps of {len(jobs)} networks in {dt:.3f} s", file=sys.stderr, flush=True)
+        if runner is not None:
+            runner.close()
+        if arm == "step_many":
+            tune = B.autotune(engines, jobs, sync)
+            best_rule = B.shape_rule(tune["blocks_per_module"])
+            extra["autotune"] = {"blocks_per_module": tune["blocks_per_module"],
+                                 "seconds_per_graph_run": {str(k): v for k, v in tune["seconds"].items()}}
         for e in engines:
             e.close()
         del engines
-    (ts, evs), (tb, evb) = res["sequential"], res["batched"]
     neurons = sum(c.glob_n for c in jobs)
+    evs = res["sequential"][1]
     print(json.dumps({
-        "metric": "aggregate synaptic events/s (batched sweep)", "value": sum(evb) / tb, "unit": UNIT,
-        "n_gpus": 1, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+        "metric": "aggregate synaptic events/s (batched sweep)", "value": sum(res["graph"][1]) / res["graph"][0],
+        "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"{len(jobs)} independent networks of 1x1-4x4 modules ({neurons} neurons), "
-                               f"{args.batch_ms} ms each, per-job seed, NuExt 1-5 Hz, AlphaC 0-2, STDP off",
+                               f"steps 1..{K} of each, per-job seed, NuExt 1-5 Hz, AlphaC 0-2, STDP off, "
+                               f"one emulated rank per module",
                    "timing": "host wall time between device synchronisations"},
-        "batched_s": tb, "sequential_s": ts, "sequential_value": sum(evs) / ts, "build_s": build_s,
-        "per_job_events_identical": evs == evb,
+        "seconds": {a: r[0] for a, r in res.items()},
+        "values": {a: sum(r[1]) / r[0] for a, r in res.items()},
+        "build_s": build_s, **extra,
+        "per_job_events_identical": all(r[1] == evs for r in res.values()),
     }), flush=True)
 
 

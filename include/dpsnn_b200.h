@@ -123,6 +123,30 @@ int dpsnn_step_many(dpsnn_engine *const *engines, uint32_t n, uint32_t nsteps);
 /* Block until all queued steps are done; reports a deferred device error. */
 int dpsnn_sync(dpsnn_engine *e);
 
+/* Graphs of batched steps.  dpsnn_graph_create records nsteps steps (a
+ * positive multiple of 80) of the n engines, queued as dpsnn_step_many
+ * queues them, into one CUDA graph; nothing runs.  Every engine must have run
+ * its first step, with kernel timing, the STDP event log and the LTP probe
+ * off.  dpsnn_graph_run advances every engine by nsteps steps in one launch,
+ * after the work already queued on the engines; later work on them follows
+ * it.  A graph encodes the engines' ring slots and step parities, so a run
+ * is refused unless every engine is at the step (mod 80) it was recorded at.
+ * The engines must outlive the graph.  No counterpart in the reference, whose
+ * process runs one network per MPI job. */
+typedef struct dpsnn_graph dpsnn_graph;
+int dpsnn_graph_create(dpsnn_engine *const *engines, uint32_t n, uint32_t nsteps, dpsnn_graph **out);
+int dpsnn_graph_run(dpsnn_graph *g);
+void dpsnn_graph_destroy(dpsnn_graph *g);
+
+/* Grid sizes (blocks) of the delivery, warp-sort and heavy-run kernels; 0
+ * restores the default (8, 8 and 16 blocks per SM, sized for a network that
+ * fills the GPU).  Every kernel loops over its work, so the results do not
+ * depend on them; a small network stepped beside others runs faster on
+ * smaller grids.  Takes effect for steps queued (or graphs recorded) after
+ * the call.  No counterpart in the reference. */
+int dpsnn_set_launch_shape(dpsnn_engine *e, uint32_t deliver_blocks, uint32_t heavy_sort_blocks,
+                           uint32_t heavy_run_blocks);
+
 /* Sizes. */
 uint32_t dpsnn_glob_n(const dpsnn_engine *e);
 uint32_t dpsnn_time_ms(const dpsnn_engine *e);        /* steps completed */

@@ -46,3 +46,42 @@ def test_batched_networks_match_alone_and_reference():
         gi, gt = gio.raster(name)
         np.testing.assert_array_equal(together[k][0], gi)
         np.testing.assert_array_equal(together[k][1], gt)
+
+
+def test_graph_runs_match_plain_steps():
+    """The batched graph (dpsnn_graph_create/run, 80 steps of every network
+    per run) gives each network the raster and event count of dpsnn_step,
+    with the launch shapes the autotuner may choose, and refuses a run at a
+    step other than the one it was recorded at."""
+    import importlib
+    B = importlib.import_module(E.__name__.rsplit(".", 1)[0] + ".batch")
+    cfgs = [CASES["small_1x1"](), CASES["small_2x2"](), small(3, 2, ms=300, seed=11, nu_ext_hz=4.0, alpha_c=0.5,
+                                                              glob_h=6)]
+    plain, ev_plain = rasters_stepped_together(cfgs, 241)
+    engines = [E.Engine(c) for c in cfgs]
+    for e, c, bpm in zip(engines, cfgs, (4, 16, 0)):   # uneven grids, defaults on the last
+        e.set_launch_shape(*B.shape_rule(bpm)(e, c))
+        e.step(1)
+    out = [([], []) for _ in cfgs]
+    for e, (ids, ts) in zip(engines, out):
+        i, t = e.spikes(0)
+        ids.append(i)
+        ts.append(t)
+    g = E.Graph(engines, 80)
+    for run in range(3):
+        g.run()
+        for e, (ids, ts) in zip(engines, out):
+            for t in range(1 + 80 * run, 81 + 80 * run):
+                i, tt = e.spikes(t)
+                ids.append(i)
+                ts.append(tt)
+    for (ids, ts), (pi, pt), e, ev in zip(out, plain, engines, ev_plain):
+        np.testing.assert_array_equal(np.concatenate(ids), pi)
+        np.testing.assert_array_equal(np.concatenate(ts), pt)
+        assert e.events_delivered() == ev and e.time_ms == 241
+    engines[0].step(1)   # now at step 242: not the recorded step modulo 80
+    with pytest.raises(E.EngineError, match="recorded at"):
+        g.run()
+    g.close()
+    for e in engines:
+        e.close()
