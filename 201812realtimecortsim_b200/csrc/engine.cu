@@ -455,6 +455,9 @@ struct Dev {
   uint2 *ev;
   uint32_t *ovf_cnt;
   uint4 *ovf;
+  double *huge_tau;                   // huge_kernel's scratch: HEAVY_MAX events per block
+  uint32_t *huge_key;
+  float *huge_val;
   uint32_t *heavy_list, *heavy_cnt;   // [4N]: neuron, event count of the warp path, then of
                                       // the block path; heavy_cnt[0..1]: their lengths
   // bath
@@ -1706,11 +1709,13 @@ __global__ void __launch_bounds__(NEURON_BLOCK) neuron_kernel(Dev d) {
 // (time, key) and writes the sorted events back into the bucket;
 // heavy_run_kernel then runs those neurons one thread each.  Neurons with
 // more events (including any beyond the bucket, in the overflow list) are
-// sorted and run by huge_kernel, one block each.
+// sorted by huge_kernel, one block each; those with at most half a bucket of
+// events go back to the bucket and run in heavy_run_kernel, the others run
+// in their block.
 #define HEAVY_WARP_MAX 256     // events a warp sorts (8 per lane)
 #define HEAVY_MAX 8192
 #define HEAVY_THREADS 256
-#define HEAVY_SMEM (HEAVY_MAX * 16)
+#define HUGE_SMEM_EVENTS 2048   // a huge neuron sorted in shared memory (32 KB); more in global scratch
 
 __device__ static inline void bitonic_sort_shared(double *tau, uint32_t *key, float *val, uint32_t n2,
                                                   uint32_t tid, uint32_t nthr, bool warp_only) {
@@ -1867,15 +1872,29 @@ __global__ void __launch_bounds__(HEAVY_SORT_THREADS, 2) heavy_sort_kernel(Dev d
   }
 }
 
-// Runs a neuron whose events heavy_sort_kernel left sorted in its bucket
-// (arrival times, then weights); same merge and arithmetic as run_neuron.
+// Runs a neuron whose events were left sorted in its bucket (arrival times,
+// then weights): the warp path's neurons, and the block path's neurons with
+// at most half a bucket of events, which huge_kernel sorts and leaves there.
+// Same merge and arithmetic as run_neuron.
+__device__ static inline bool huge_runs_here(const NetConst *net, uint32_t cnt) {
+  return cnt <= net->ev_cap / 2 && cnt <= MAX_INPUTS_PER_STEP;
+}
+
 __global__ void heavy_run_kernel(Dev d) {
   const NetConst *net = d.net;
   const uint32_t t = *d.t, N = net->N, cap = net->ev_cap, wmax = warp_path_max(net);
-  const uint32_t nh = min(d.heavy_cnt[0], N);
+  const uint32_t nh0 = min(d.heavy_cnt[0], N), nh = nh0 + min(d.heavy_cnt[1], N);
   for (uint32_t hh = blockIdx.x * blockDim.x + threadIdx.x; hh < nh; hh += gridDim.x * blockDim.x) {
-    const uint32_t i = d.heavy_list[hh], ns = d.heavy_list[N + hh];
-    if (ns > wmax) continue;
+    uint32_t i, ns;
+    if (hh < nh0) {
+      i = d.heavy_list[hh];
+      ns = d.heavy_list[N + hh];
+      if (ns > wmax) continue;
+    } else {
+      i = d.heavy_list[2ull * N + (hh - nh0)];
+      ns = d.heavy_list[3ull * N + (hh - nh0)];
+      if (ns <= wmax || !huge_runs_here(net, ns)) continue;
+    }
     const uint2 *ev = d.ev + (size_t)i * cap;
     const double *st = reinterpret_cast<const double *>(ev);
     const float *sv = reinterpret_cast<const float *>(ev + cap / 2);
@@ -1913,10 +1932,12 @@ __device__ static inline uint32_t gather_events(const Dev &d, uint32_t i, uint32
 }
 
 __global__ void __launch_bounds__(HEAVY_THREADS) huge_kernel(Dev d) {
-  extern __shared__ __align__(16) unsigned char heavy_smem_raw[];
-  double *s_tau = reinterpret_cast<double *>(heavy_smem_raw);
-  uint32_t *s_key = reinterpret_cast<uint32_t *>(s_tau + HEAVY_MAX);
-  float *s_val = reinterpret_cast<float *>(s_key + HEAVY_MAX);
+  // 32 KB of shared memory, so that a block fits on an SM beside the bath's
+  // blocks; the rare neuron with more events sorts in its block's global
+  // scratch (HEAVY_MAX events)
+  __shared__ double sh_tau[HUGE_SMEM_EVENTS];
+  __shared__ uint32_t sh_key[HUGE_SMEM_EVENTS];
+  __shared__ float sh_val[HUGE_SMEM_EVENTS];
   __shared__ uint32_t s_n;
   const NetConst *net = d.net;
   const uint32_t t = *d.t, N = net->N, D = net->D, tid = threadIdx.x;
@@ -1929,7 +1950,12 @@ __global__ void __launch_bounds__(HEAVY_THREADS) huge_kernel(Dev d) {
       if (tid == 0) atomicOr(d.flags, F_TOO_MANY_INPUTS);
       continue;
     }
-    const uint32_t n = gather_events(d, i, cnt, s_key, s_val, HEAVY_MAX, tid, blockDim.x, &s_n);
+    const bool in_smem = cnt <= HUGE_SMEM_EVENTS;
+    double *s_tau = in_smem ? sh_tau : d.huge_tau + (size_t)blockIdx.x * HEAVY_MAX;
+    uint32_t *s_key = in_smem ? sh_key : d.huge_key + (size_t)blockIdx.x * HEAVY_MAX;
+    float *s_val = in_smem ? sh_val : d.huge_val + (size_t)blockIdx.x * HEAVY_MAX;
+    const uint32_t n = gather_events(d, i, cnt, s_key, s_val, in_smem ? HUGE_SMEM_EVENTS : HEAVY_MAX, tid,
+                                     blockDim.x, &s_n);
     uint32_t n2 = 1;
     while (n2 < n) n2 <<= 1;
     for (uint32_t e = tid; e < n2; e += blockDim.x) {
@@ -1942,7 +1968,17 @@ __global__ void __launch_bounds__(HEAVY_THREADS) huge_kernel(Dev d) {
     }
     __syncthreads();
     bitonic_sort_shared(s_tau, s_key, s_val, n2, tid, blockDim.x, false);
-    if (tid == 0) {
+    if (huge_runs_here(net, cnt)) {
+      // sorted back into the bucket's halves; heavy_run_kernel runs the
+      // neuron, beside the others, one thread each
+      uint2 *ev = d.ev + (size_t)i * net->ev_cap;
+      double *st = reinterpret_cast<double *>(ev);
+      float *sv = reinterpret_cast<float *>(ev + net->ev_cap / 2);
+      for (uint32_t e = tid; e < n; e += blockDim.x) {
+        st[e] = s_tau[e];
+        sv[e] = s_val[e];
+      }
+    } else if (tid == 0) {
       if (run_neuron(d, i, t, s_tau, s_val, n)) atomicAdd(&d.block_fired[i / NEURON_BLOCK], 1u);
     }
     __syncthreads();
@@ -2531,6 +2567,13 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
   DALLOC(d.ovf_cnt, 1);
   DALLOC(d.ovf, n.ovf_cap);
   DALLOC(d.heavy_list, 4ull * N);
+  {   // huge_kernel's global scratch: one neuron of up to HEAVY_MAX events per block
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e->device);
+    DALLOC(d.huge_tau, (size_t)nsm * HEAVY_MAX);
+    DALLOC(d.huge_key, (size_t)nsm * HEAVY_MAX);
+    DALLOC(d.huge_val, (size_t)nsm * HEAVY_MAX);
+  }
   DALLOC(d.heavy_cnt, 2);
   DALLOC(d.t, 1);
   DALLOC(d.bath_t, 1);
@@ -2623,7 +2666,11 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
   e->grid_heavy_run = (uint32_t)sms * 16;
   e->grid_huge = (uint32_t)sms;
   CK(cudaFuncSetAttribute(bath_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(BathSmem)));
-  CK(cudaFuncSetAttribute(huge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, HEAVY_SMEM));
+  // the bath's blocks stay resident for most of a step: with the largest
+  // shared-memory carveout, the SMs that hold two of them still have room for
+  // a block of the main stream's kernels that use shared memory
+  CK(cudaFuncSetAttribute(bath_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                          (int)cudaSharedmemCarveoutMaxShared));
   free_temps(e);   // after their last use on this stream
   CK(cudaStreamSynchronize(e->stream));
   return 0;
@@ -2824,12 +2871,12 @@ static int enqueue_step(dpsnn_engine *e) {
   timed_launch_begin(e, 5);
   heavy_sort_kernel<<<e->grid_heavy, HEAVY_SORT_THREADS, 0, e->stream>>>(d);
   timed_launch_end(e, 5);
+  timed_launch_begin(e, 7);
+  huge_kernel<<<e->grid_huge, HEAVY_THREADS, 0, e->stream>>>(d);
+  timed_launch_end(e, 7);
   timed_launch_begin(e, 6);
   heavy_run_kernel<<<e->grid_heavy_run, 128, 0, e->stream>>>(d);
   timed_launch_end(e, 6);
-  timed_launch_begin(e, 7);
-  huge_kernel<<<e->grid_huge, HEAVY_THREADS, HEAVY_SMEM, e->stream>>>(d);
-  timed_launch_end(e, 7);
   cudaEventRecord(e->ev_neuron[b], e->stream);
   if (e->hnet.stdp_on) {
     if (d.probe_w && t % 1000 == 999 && t >= e->hnet.start_pl && t <= e->hnet.stop_pl) e->probe_t = t;
@@ -2878,6 +2925,16 @@ extern "C" int dpsnn_step_many(dpsnn_engine *const *engines, uint32_t n, uint32_
 // A graph encodes the engines' ring slots and step parities, so it runs only
 // when every engine is at the step (mod 80) it was recorded at; nsteps is a
 // multiple of 80, so consecutive runs chain.
+// The events that order an engine's two streams between steps, recorded at
+// the streams' current ends: after a graph run (whose own copies of them are
+// internal to the graph) later steps wait on everything before.
+static void rearm_step_events(dpsnn_engine *e) {
+  for (int b = 0; b < 2; b++) {
+    cudaEventRecord(e->ev_neuron[b], e->stream);
+    cudaEventRecord(e->ev_bath[b], e->bath_stream);
+  }
+}
+
 struct dpsnn_graph {
   std::vector<dpsnn_engine *> engines;
   std::vector<uint32_t> t0;        // each engine's step (mod RING_SLOTS) at recording
@@ -2972,6 +3029,9 @@ extern "C" int dpsnn_graph_create(dpsnn_engine *const *engines, uint32_t n, uint
     e->launches = l_saved[i];
   }
   err = cudaStreamEndCapture(g->stream, &g->graph);
+  // the streams' order events were last recorded inside the capture: record
+  // them again outside it, so that plain steps can wait on them (no step ran)
+  for (uint32_t i = 0; i < n; i++) rearm_step_events(engines[i]);
   if (rc) return fail(rc);
   if (err != cudaSuccess) return fail(dpsnn_fail(DPSNN_E_CUDA, "cudaStreamEndCapture: %s", cudaGetErrorString(err)));
   err = cudaGraphInstantiate(&g->exec, g->graph, 0);
@@ -3001,6 +3061,7 @@ extern "C" int dpsnn_graph_run(dpsnn_graph *g) {
     dpsnn_engine *e = g->engines[i];
     CK(cudaStreamWaitEvent(e->stream, g->done, 0));
     CK(cudaStreamWaitEvent(e->bath_stream, g->done, 0));
+    rearm_step_events(e);
     e->t_host += g->nsteps;
   }
   g->engines[0]->launches += g->launches_per_run;   // counted on the first engine
@@ -3041,7 +3102,7 @@ extern "C" uint64_t dpsnn_events_delivered(const dpsnn_engine *e) {
 extern "C" int dpsnn_spikes(dpsnn_engine *e, uint32_t t_ms, uint32_t *ids, double *te, uint32_t cap,
                             uint32_t *count) {
   if (!e || !count) return dpsnn_fail(DPSNN_E_PARAM, "null argument");
-  if (t_ms >= e->t_host || t_ms + RING_SLOTS <= e->t_host)
+  if (t_ms >= e->t_host || t_ms + RING_SLOTS < e->t_host)
     return dpsnn_fail(DPSNN_E_STATE, "step %u is not among the last %d completed steps", t_ms, RING_SLOTS);
   cudaSetDevice(e->device);
   const uint32_t slot = t_ms % RING_SLOTS;
@@ -3071,7 +3132,7 @@ extern "C" int dpsnn_spikes_range(dpsnn_engine *e, uint32_t t0, uint32_t n, uint
                                   uint64_t cap, uint32_t *counts) {
   if (!e || !counts || (n && (!ids || !te))) return dpsnn_fail(DPSNN_E_PARAM, "null argument");
   if (n == 0) return 0;
-  if (n > RING_SLOTS || t0 + n > e->t_host || t0 + RING_SLOTS <= e->t_host)
+  if (n > RING_SLOTS || t0 + n > e->t_host || t0 + RING_SLOTS < e->t_host)
     return dpsnn_fail(DPSNN_E_STATE, "steps %u..%u are not among the last %d completed steps", t0, t0 + n - 1,
                       RING_SLOTS);
   cudaSetDevice(e->device);
@@ -3409,7 +3470,7 @@ extern "C" int dpsnn_rank_spikes_noalloc(dpsnn_engine *e, uint32_t t_ms, uint32_
   if (e->hnet.locN > DPSNN_NOALLOC_MAX_SPIKES)
     return dpsnn_fail(DPSNN_E_CAPACITY, "rank of %u neurons exceeds the %d-spike scratch of dpsnn_rank_spikes_noalloc",
                       e->hnet.locN, DPSNN_NOALLOC_MAX_SPIKES);
-  if (t_ms >= e->t_host || t_ms + RING_SLOTS <= e->t_host)
+  if (t_ms >= e->t_host || t_ms + RING_SLOTS < e->t_host)
     return dpsnn_fail(DPSNN_E_STATE, "step %u is not among the last %d completed steps", t_ms, RING_SLOTS);
   cudaSetDevice(e->device);
   NoAllocScratch *s = nullptr;

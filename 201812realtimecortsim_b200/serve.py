@@ -84,7 +84,7 @@ def estimate_device_bytes(cfg: nc.NetConfig, events_per_neuron: int = 1024) -> i
             max_ext = max(max_ext, math.ceil(20 / inv))
     per_neuron = 66 + 2 * (cfg.D + 1) + 8 + 80 * 12 + 8 * cap + 20 + 12 + 2 * 9 * max_ext + 2 * 2 * cfg.D + 4
     per_syn = 6 + (12 if cfg.stdp is not None else 0)
-    fixed = (96 << 20) + cfg.glob_h * 90_000 + cfg.n_modules * 2 * 7500 * 4
+    fixed = (116 << 20) + cfg.glob_h * 90_000 + cfg.n_modules * 2 * 7500 * 4
     return int(N * per_neuron + 1.1 * expected_synapses(cfg) * per_syn + fixed)
 
 
