@@ -9,7 +9,9 @@
 //    results (device code is compiled with --fmad=false, host code with
 //    -ffp-contract=off).  exp: argument reduction by k*ln2, a Taylor series
 //    on r/256 and eight squarings.  log: x = 2^e*m, m in [0.75,1.5), table
-//    point c = round(64 m)/64, log m = log c + 2 atanh((m-c)/(m+c)).
+//    point c = round(64 m)/64, log m = log c + 2 atanh((m-c)/(m+c)); a short
+//    evaluation with an error bound decides the rounding, the full series
+//    only when it cannot.
 //    The C library's exp/log differ from the correctly rounded value in about
 //    0.08% of arguments by one ulp; the raster is bit-identical to the
 //    reference until such a difference first changes a threshold decision.
@@ -108,8 +110,8 @@ DD_HD double exp_cr(double x) {
   return ldexp(ldexp(e.hi + e.lo, k1), k2);
 }
 
-// Correctly rounded log(x) for x > 0.
-DD_HD double log_cr(double x) {
+// Correctly rounded log(x) for x > 0: the full double-double series.
+DD_HD double log_cr_dd(double x) {
   if (!(x > 0.0)) return (x == 0.0) ? -INFINITY : NAN;
   if (x == INFINITY) return x;
   int e = 0;
@@ -135,6 +137,47 @@ DD_HD double log_cr(double x) {
     res = dd_add(el, res);
   }
   return res.hi + res.lo;
+}
+
+// Correctly rounded log(x) for x > 0.  The same reduction as log_cr_dd, but
+// only the leading terms in double-double: 2s with s = (m-c)/(m+c) to about
+// 2^-104, the table's log c and e*ln2; the rest of the atanh series
+// (|s| < 0.0053, terms through s^13, the first omitted one below 2^-108 of
+// 2|s|) in double.  The result carries an error bound; when both ends of it
+// round to the same double that double is the correctly rounded log, else
+// log_cr_dd decides (rare: the bound is about 2^-95 of the terms' size).
+DD_HD double log_cr(double x) {
+  if (!(x > 0.0)) return (x == 0.0) ? -INFINITY : NAN;
+  if (x == INFINITY) return x;
+  int e = 0;
+  double m = frexp(x, &e);   // m in [0.5,1)
+  m *= 2.0;
+  e -= 1;                    // m in [1,2)
+  if (m >= 1.5) { m *= 0.5; e += 1; }
+  const double j = rint(m * 64.0);      // 48..96
+  const double c = j * 0x1p-6;
+  const double rn = m - c;              // exact
+  const dd_t den = two_sum(m, c);
+  const double sh = rn / den.hi;
+  const dd_t p = two_prod(sh, den.hi);
+  const double sl = (((rn - p.hi) - p.lo) - sh * den.lo) / den.hi;
+  const double s2 = sh * sh;
+  const double tail =
+      sh * s2 *
+      (2.0 / 3 + s2 * (2.0 / 5 + s2 * (2.0 / 7 + s2 * (2.0 / 9 + s2 * (2.0 / 11 + s2 * (2.0 / 13))))));
+  const dd_t at = two_sum(2.0 * sh, 2.0 * sl + tail);
+  const dd_t lc = dd_tab(DD_TAB(dd_log_j64), (int)j - 48);
+  dd_t res = dd_add(lc, at);
+  double mag = fabs(lc.hi) + fabs(at.hi);
+  if (e != 0) {
+    const dd_t el = dd_add(two_prod((double)e, DD_LN2_HI), two_prod((double)e, DD_LN2_LO));
+    res = dd_add(el, res);
+    mag += fabs(el.hi);
+  }
+  const double err = mag * 0x1p-95 + fabs(tail) * 0x1p-48;
+  const double lo = res.hi + (res.lo - err), hi = res.hi + (res.lo + err);
+  if (lo == hi) return lo;
+  return log_cr_dd(x);
 }
 
 // Fix-up table of the C library's logf on (0,1]: sorted input bit patterns

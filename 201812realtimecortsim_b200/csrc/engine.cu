@@ -472,6 +472,8 @@ struct Dev {
   uint8_t *bath_lut;
   logf_fixup_t fix;
   const uint32_t *fix_bitmap; // one bit per float in [0x30000000, 0x3F800000]: key has a fix-up
+  const float *fix_near;      // [256] by the result's exponent: a fix-up input's exact log lies at most
+                              // this many ulps from a rounding midpoint (-1: none in that binade)
   // control
   uint32_t *t;              // current step
   uint32_t *bath_t;         // step of the next bath launch (the bath runs one step ahead)
@@ -724,10 +726,11 @@ __global__ void __launch_bounds__(DELIVER_THREADS) deliver_kernel(Dev d) {
 //              around the prediction (a warp per neuron, two candidates per
 //              lane) a binary search of q[] finds c (c - 1 sums below the
 //              lower bound, the c-th at or above the upper one); a candidate
-//              the bounds do not decide is marked undecided.  The builders
-//              then compose the tables: for every candidate start of neuron
-//              2p the events of neurons 2p and 2p+1 together, then of 4k ..
-//              4k+3 together;
+//              the bounds do not decide is marked undecided.  A builder
+//              takes whole quads of neurons (the rank's quads in turn) and
+//              composes their tables itself: for every candidate start of
+//              neuron 2p the events of neurons 2p and 2p+1 together, then of
+//              4k .. 4k+3 together;
 //   warp 0     (walk) follows the chain: one lookup per four neurons, at the
 //              quad's actual start, gives the next quad's start.  A quad the
 //              tables do not decide goes neuron by neuron, and an undecided
@@ -779,8 +782,7 @@ struct BathSmem {
   uint8_t tab2[BATH_TABS][16][BATH_TROW];
   uint8_t tab4[BATH_TABS][8][BATH_TROW];
   uint32_t bp_base[BATH_TABS][32];  // position (low 32 bits) of candidate 0 of neuron j
-  uint32_t tab_cnt[BATH_TABS];      // builder-warp completions of the tables of this buffer
-  uint32_t bld_sync;                // builder-warp arrivals at the table stages
+  uint32_t tab_cnt[BATH_TABS];      // quads whose tables of this buffer are complete
   uint32_t c_start[32], c_cnt[32];  // the walk's record: quad starts, and neurons walked one by one
   uint32_t e_start[2][32], e_cnt[2][32];  // chunk c, handed to the emitter in buffer c & 1
   unsigned long long e_end[2];      // its end position
@@ -806,14 +808,26 @@ __device__ __forceinline__ uint32_t bath_row(uint32_t dl) {
   return min(__funnelshift_r(dl, dl, 1), (uint32_t)BATH_NC);
 }
 
-// logf of the host C library on (0,1]: a one-bit-per-float filter, then a
-// binary search of the fix-up keys.
-__device__ static inline float logf_ref_dev(const logf_fixup_t &fx, const uint32_t *__restrict__ bitmap, float x) {
-  const float f = logf_cr_from(x, log((double)x));
+// logf of the host C library on (0,1].  The inputs where it differs from
+// the correctly rounded float all have an exact logarithm close to a
+// rounding midpoint; an input whose logarithm lies farther from one than any
+// fix-up input of the same result binade returns the correctly rounded value
+// at once.  Otherwise a one-bit-per-float filter, then a binary search of
+// the fix-up keys.
+__device__ static inline float logf_ref_dev(const logf_fixup_t &fx, const uint32_t *__restrict__ bitmap,
+                                            const float *__restrict__ near, float x) {
+  const double y = log((double)x);
+  const float f = logf_cr_from(x, y);
   union { float f; uint32_t u; } b;
   b.f = x;
   const uint32_t key = b.u;
   if (key < 0x30000000u || key > 0x3F800000u) return f;
+  const uint32_t fb = __float_as_uint(f), E = (fb >> 23) & 0xFFu;
+  if ((fb & 0x7FFFFFu) != 0 && E > 24) {   // not a power of two: one ulp on either side
+    const double inv_ulp = __longlong_as_double((long long)(150 - E + 1023) << 52);   // 2^(150-E)
+    const double dist = 0.5 - fabs(y - (double)f) * inv_ulp;
+    if (dist > (double)__ldg(&near[E])) return f;
+  }
   const uint32_t bit = key - 0x30000000u;
   if (!((__ldg(&bitmap[bit >> 5]) >> (bit & 31)) & 1u)) return f;
   uint32_t lo = 0, hi = fx.n;
@@ -831,7 +845,7 @@ __device__ static inline float bath_lapse(const Dev &d, uint32_t mj, uint8_t &id
   idx = (uint8_t)(uint32_t)(u * 256);
   double temp = (double)1.0 - u;
   if (temp < 0) temp = 0;
-  return -logf_ref_dev(d.fix, d.fix_bitmap, (float)temp);
+  return -logf_ref_dev(d.fix, d.fix_bitmap, d.fix_near, (float)temp);
 }
 
 __device__ static inline uint32_t lap_fixed(float lap) {
@@ -912,32 +926,11 @@ __device__ static inline unsigned long long bath_exact(BathSmem &s, double nbv, 
   return pos;
 }
 
-// The builder warps' meeting between table stages: each warp arrives, then
-// waits (bounded) until all BATH_BUILDERS have arrived `stage` times.  False
-// when the block is stopping.  Lane 0 waits; the answer is the warp's.
-__device__ static inline bool bath_builders_meet(BathSmem &s, uint32_t stage, uint32_t lane) {
-  volatile BathSmem &vs = s;
-  __syncwarp();
-  __threadfence_block();
-  bool ok = true;
-  if (lane == 0) {
-    atomicAdd(&s.bld_sync, 1u);
-    uint32_t sp = 0;
-    while (vs.bld_sync < BATH_BUILDERS * stage) {
-      if (vs.done) { ok = false; break; }
-      if (++sp > BATH_SPIN_LIMIT) { vs.err = 1; vs.done = 1; ok = false; break; }
-    }
-  }
-  ok = __shfl_sync(0xffffffffu, ok, 0);
-  __threadfence_block();
-  return ok;
-}
-
 __device__ static inline int bath_builder_index(uint32_t warp) {
   return (warp >= 5 && warp <= 7) ? (int)warp - 5 : (warp >= 9 && warp <= 11) ? (int)warp - 6 : -1;
 }
 
-__global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
+__global__ void __launch_bounds__(BATH_THREADS, 2) bath_kernel(Dev d) {
   const uint32_t t = *d.bath_t;
   extern __shared__ __align__(16) unsigned char bath_smem_raw[];
   BathSmem &s = *reinterpret_cast<BathSmem *>(bath_smem_raw);
@@ -963,7 +956,6 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
     s.done = 0;
     s.err = 0;
     s.chunk_seq = 0;
-    s.bld_sync = 0;
     s.e_seq = 0;
     s.emit_done = 0;
     s.emit_pos = p0;
@@ -1081,10 +1073,6 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
       // candidate o of this lane's neuron starts at base + 2o, the
       // prediction in the middle of the window
       const unsigned long long base = pred + 2ull * (incl - ec) - BATH_NC;
-      if (bw == 0) {
-        s.bp_base[b][lane] = (uint32_t)base;
-        *reinterpret_cast<uint32_t *>(&s.tab[b][lane][BATH_NC]) = misc ? 0xFFFFFFFFu : 0u;
-      }
       // the draws every candidate of the chunk reads are converted; never
       // beyond what the generator may produce ahead of the walk (once the
       // emitter is done with the chunks before c-2, at least floor_pos +
@@ -1111,17 +1099,20 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
         }
       }
       if (fail) break;
-      // stage 1, this warp's neurons j = bw, bw + BATH_BUILDERS, ..; for
-      // neuron j the lanes take the candidates o = lane and lane + 32.  For
-      // a start P the count is m + 1, m the number of k < 32 whose sum of
-      // the k+1 lapses at P+1, P+3, .., P+1+2k is below lo (the sums grow
-      // with k), when the (m+1)-th sum reaches hi1.  Positions are taken
-      // modulo 2^32 (a step reads far fewer draws); the two candidates'
-      // binary searches run in lockstep.
-      {
-        const uint32_t b32 = (uint32_t)base, f32 = (uint32_t)floor_pos;
-        const uint32_t r32 = (uint32_t)reach - BATH_WINDOW;
-        for (uint32_t j = bw; j < 32; j += BATH_BUILDERS) {
+      const uint32_t b32 = (uint32_t)base, f32 = (uint32_t)floor_pos;
+      const uint32_t r32 = (uint32_t)reach - BATH_WINDOW;
+      // this warp's quads of the chunk: the rank's quads go to the builders
+      // in turn (quad 8c + k to builder (8c + k) mod BATH_BUILDERS), so each
+      // builder takes four quads in three chunks and needs no other warp
+      for (uint32_t k = (bw + BATH_BUILDERS - (8 * c) % BATH_BUILDERS) % BATH_BUILDERS; k < 8; k += BATH_BUILDERS) {
+        // stage 1: the quad's neurons j = 4k .. 4k+3; for neuron j the lanes
+        // take the candidates o = lane and lane + 32.  For a start P the
+        // count is m + 1, m the number of i < 32 whose sum of the i+1
+        // lapses at P+1, P+3, .., P+1+2i is below lo (the sums grow with
+        // i), when the (m+1)-th sum reaches hi1.  Positions are taken
+        // modulo 2^32 (a step reads far fewer draws); the two candidates'
+        // binary searches run in lockstep.
+        for (uint32_t j = 4 * k; j < 4 * k + 4; j++) {
           const uint32_t mj = __shfl_sync(0xffffffffu, misc, j);
           const uint32_t loj = __shfl_sync(0xffffffffu, lo, j), hij = __shfl_sync(0xffffffffu, hi1, j);
           const uint32_t bj = __shfl_sync(0xffffffffu, b32, j);
@@ -1132,68 +1123,81 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
             continue;
           }
           const uint32_t cap = mj & 0xFFu;
-          uint32_t P[2], qb[2], m[2];
+          // draw P+1+2i of a candidate sits at word hv | ((w0 + i) mod 4096) of q[]
+          const uint32_t hv = ((bj + 1) & 1u) * (BATH_RING / 2);
+          uint32_t w0[2], qb[2], m[2];
           bool ok[2];
 #pragma unroll
           for (int v = 0; v < 2; v++) {
-            P[v] = bj + 2u * (lane + 32u * v);
-            ok[v] = (int32_t)(P[v] - f32) >= 0 && (int32_t)(r32 - P[v]) >= 0;
-            qb[v] = s.q[bath_qi(P[v] - 1)];
+            const uint32_t P = bj + 2u * (lane + 32u * v);
+            ok[v] = (int32_t)(P - f32) >= 0 && (int32_t)(r32 - P) >= 0;
+            w0[v] = (P + 1) >> 1;
+            qb[v] = s.q[hv | ((w0[v] - 1) & (BATH_RING / 2 - 1))];
             m[v] = 0;
           }
 #pragma unroll
           for (uint32_t st = 16; st > 0; st >>= 1) {
             uint32_t f[2];
 #pragma unroll
-            for (int v = 0; v < 2; v++) f[v] = s.q[bath_qi(P[v] + 1 + 2 * (m[v] + st - 1))];
+            for (int v = 0; v < 2; v++) f[v] = s.q[hv | ((w0[v] + m[v] + st - 1) & (BATH_RING / 2 - 1))];
 #pragma unroll
             for (int v = 0; v < 2; v++) m[v] += (f[v] - qb[v] < loj) ? st : 0u;
           }
 #pragma unroll
           for (int v = 0; v < 2; v++) {
-            const uint32_t F = s.q[bath_qi(P[v] + 1 + 2 * m[v])] - qb[v];
+            const uint32_t F = s.q[hv | ((w0[v] + m[v]) & (BATH_RING / 2 - 1))] - qb[v];
             const uint32_t mm = (m[v] == 31 && F < loj) ? 32u : m[v];
             row[lane + 32 * v] = (ok[v] && mm < cap && F >= hij) ? (uint8_t)(mm + 1) : (uint8_t)0xFF;
           }
         }
-      }
-      // the composed tables' answers outside the window: 0 when none of
-      // their neurons has an event, else undecided
-      if (bw == 0) {
-        const uint32_t m2 = __shfl_sync(0xffffffffu, misc, (2 * lane) & 31) |
-                            __shfl_sync(0xffffffffu, misc, (2 * lane + 1) & 31);
-        const uint32_t m4 = __shfl_sync(0xffffffffu, m2, (2 * lane) & 31) |
-                            __shfl_sync(0xffffffffu, m2, (2 * lane + 1) & 31);
-        if (lane < 16) *reinterpret_cast<uint32_t *>(&s.tab2[b][lane][BATH_NC]) = m2 ? 0xFFFFFFFFu : 0u;
-        if (lane < 8) *reinterpret_cast<uint32_t *>(&s.tab4[b][lane][BATH_NC]) = m4 ? 0xFFFFFFFFu : 0u;
-      }
-      if (!bath_builders_meet(s, 2 * c + 1, lane)) { fail = true; break; }
-      // stage 2: pairs, from each candidate start of neuron 2p through 2p+1
-      for (uint32_t e = bw * 32 + lane; e < 16 * BATH_NC; e += 32 * BATH_BUILDERS) {
-        const uint32_t pp = e / BATH_NC, o = e % BATH_NC, a = 2 * pp;
-        const uint32_t ca = s.tab[b][a][o];
-        uint32_t v = 0xFFu;
-        if (ca != 0xFFu) {
-          const uint32_t cb = s.tab[b][a + 1][bath_row(s.bp_base[b][a] + 2 * (o + ca) - s.bp_base[b][a + 1])];
-          if (cb != 0xFFu) v = ca + cb;
+        // the quad's window bases, and each table's answer outside its
+        // window: 0 when none of its neurons has an event, else undecided
+        const uint32_t mq = __shfl_sync(0xffffffffu, misc, 4 * k + (lane & 3));
+        const uint32_t bq = __shfl_sync(0xffffffffu, b32, 4 * k + (lane & 3));
+        const uint32_t B0 = __shfl_sync(0xffffffffu, b32, 4 * k), B1 = __shfl_sync(0xffffffffu, b32, 4 * k + 1);
+        const uint32_t B2 = __shfl_sync(0xffffffffu, b32, 4 * k + 2), B3 = __shfl_sync(0xffffffffu, b32, 4 * k + 3);
+        const uint32_t m2a = __shfl_sync(0xffffffffu, mq, 0) | __shfl_sync(0xffffffffu, mq, 1);
+        const uint32_t m2b = __shfl_sync(0xffffffffu, mq, 2) | __shfl_sync(0xffffffffu, mq, 3);
+        if (lane < 4) {
+          s.bp_base[b][4 * k + lane] = bq;
+          *reinterpret_cast<uint32_t *>(&s.tab[b][4 * k + lane][BATH_NC]) = mq ? 0xFFFFFFFFu : 0u;
         }
-        s.tab2[b][pp][o] = (uint8_t)v;
-      }
-      if (!bath_builders_meet(s, 2 * c + 2, lane)) { fail = true; break; }
-      // stage 3: quads, from each candidate start of neuron 4k through its two pairs
-      for (uint32_t e = bw * 32 + lane; e < 8 * BATH_NC; e += 32 * BATH_BUILDERS) {
-        const uint32_t k = e / BATH_NC, o = e % BATH_NC, a = 4 * k;
-        const uint32_t va = s.tab2[b][2 * k][o];
-        uint32_t v = 0xFFu;
-        if (va != 0xFFu) {
-          const uint32_t vb = s.tab2[b][2 * k + 1][bath_row(s.bp_base[b][a] + 2 * (o + va) - s.bp_base[b][a + 2])];
-          if (vb != 0xFFu) v = va + vb;   // at most 4 x 32
+        if (lane == 0) {
+          *reinterpret_cast<uint32_t *>(&s.tab2[b][2 * k][BATH_NC]) = m2a ? 0xFFFFFFFFu : 0u;
+          *reinterpret_cast<uint32_t *>(&s.tab2[b][2 * k + 1][BATH_NC]) = m2b ? 0xFFFFFFFFu : 0u;
+          *reinterpret_cast<uint32_t *>(&s.tab4[b][k][BATH_NC]) = (m2a | m2b) ? 0xFFFFFFFFu : 0u;
         }
-        s.tab4[b][k][o] = (uint8_t)v;
+        __syncwarp();
+        // stage 2: the two pairs, from each candidate start of neuron 2p through 2p+1
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+          const uint32_t pp = 2 * k + (v >> 1), o = lane + 32u * (v & 1), a = 2 * pp;
+          const uint32_t ba = (v >> 1) ? B2 : B0, bn = (v >> 1) ? B3 : B1;
+          const uint32_t ca = s.tab[b][a][o];
+          uint32_t val = 0xFFu;
+          if (ca != 0xFFu) {
+            const uint32_t cb = s.tab[b][a + 1][bath_row(ba + 2 * (o + ca) - bn)];
+            if (cb != 0xFFu) val = ca + cb;
+          }
+          s.tab2[b][pp][o] = (uint8_t)val;
+        }
+        __syncwarp();
+        // stage 3: the quad, from each candidate start of neuron 4k through its two pairs
+#pragma unroll
+        for (int v = 0; v < 2; v++) {
+          const uint32_t o = lane + 32u * v;
+          const uint32_t va = s.tab2[b][2 * k][o];
+          uint32_t val = 0xFFu;
+          if (va != 0xFFu) {
+            const uint32_t vb = s.tab2[b][2 * k + 1][bath_row(B0 + 2 * (o + va) - B2)];
+            if (vb != 0xFFu) val = va + vb;   // at most 4 x 32
+          }
+          s.tab4[b][k][o] = (uint8_t)val;
+        }
+        __syncwarp();
+        __threadfence_block();
+        if (lane == 0) atomicAdd(&s.tab_cnt[b], 1u);
       }
-      __syncwarp();
-      __threadfence_block();
-      if (lane == 0) atomicAdd(&s.tab_cnt[b], 1u);
       if (c0 + 32 < locN) prepare(c0 + 32);
     }
   } else if (warp == 2 || warp == 3) {
@@ -1282,7 +1286,7 @@ __global__ void __launch_bounds__(BATH_THREADS) bath_kernel(Dev d) {
       // this chunk's count tables, then its start for the builders
       {
         uint32_t sp = 0;
-        while (vs.tab_cnt[tb] < BATH_BUILDERS * (ck / BATH_TABS + 1)) {
+        while (vs.tab_cnt[tb] < 8u * (ck / BATH_TABS + 1)) {
           if (vs.done || ++sp > BATH_SPIN_LIMIT) { fail = true; break; }
           __nanosleep(20);   // leave the shared-memory pipe to the builders
         }
@@ -1759,17 +1763,27 @@ __device__ static inline uint32_t warp_path_max(const NetConst *net) {
 // bucket's size, spread over the lanes.
 #define HS_BUCKETS 256
 
+#define HS_BATH_MAX 128         // bath events a warp merges into the sorted stream
+
 struct HeavySortWarp {
   uint32_t start[HS_BUCKETS + 1];   // counts, then the buckets' first positions
   double tau[HEAVY_WARP_MAX];       // events staged by bucket for the counts
   uint32_t key[HEAVY_WARP_MAX];
+  double btau[HS_BATH_MAX];         // the neuron's bath events (time-ordered)
 };
+
+// A heavy neuron's merged event stream in its bucket: {time, input} per
+// event, synaptic and bath events in the order the reference merges them
+// (mergeFunction, DPSNN_neuron_sim.c:391-421: a synaptic event first on
+// equal times).  The list's count entry carries this flag when the sort
+// left the stream merged.
+#define HEAVY_MERGED 0x80000000u
 
 // One heavy neuron's n <= 32*E events (element e = lane + 32r in register r):
 // loaded with their arrival times, sorted by (time, key), written back as
 // sorted times into the bucket's first half and weights into its second half.
 template <int E>
-__device__ static inline void heavy_sort_one(const Dev &d, uint2 *ev, uint32_t n, uint32_t t, uint32_t D,
+__device__ static inline bool heavy_sort_one(const Dev &d, uint32_t i, uint2 *ev, uint32_t n, uint32_t t, uint32_t D,
                                              uint32_t N, uint32_t cap, uint32_t lane, HeavySortWarp &w) {
   const double T0 = (double)t;
   for (uint32_t b = lane; b <= HS_BUCKETS; b += 32) w.start[b] = 0;
@@ -1824,6 +1838,15 @@ __device__ static inline void heavy_sort_one(const Dev &d, uint2 *ev, uint32_t n
     }
   }
   __syncwarp();
+  // the merged stream when it fits half the bucket (16 B per event), else
+  // sorted times and weights in the bucket's halves (heavy_run merges)
+  const uint32_t bc = d.bath_cnt[i];
+  const uint64_t bbase = d.bath_rank_base[i / d.net->locN] + d.bath_off[i];
+  const bool merged = n + bc <= cap / 2 && bc <= HS_BATH_MAX;
+  if (merged)
+    for (uint32_t j = lane; j < bc; j += 32) w.btau[j] = d.bath_time[bbase + j];
+  __syncwarp();
+  double2 *ms = reinterpret_cast<double2 *>(ev);
   double *st = reinterpret_cast<double *>(ev);
   float *sv = reinterpret_cast<float *>(ev + cap / 2);
 #pragma unroll
@@ -1838,11 +1861,31 @@ __device__ static inline void heavy_sort_one(const Dev &d, uint2 *ev, uint32_t n
         const double tj = w.tau[j];
         rank += (tj < tm) || (tj == tm && w.key[j] < k);
       }
-      st[b0 + rank] = tm;
-      sv[b0 + rank] = __uint_as_float(x[r].y);
+      if (merged) {   // after the bath events strictly before it
+        uint32_t lo = 0, hi = bc;
+        while (lo < hi) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if (w.btau[mid] < tm) lo = mid + 1; else hi = mid;
+        }
+        ms[b0 + rank + lo] = make_double2(tm, (double)__uint_as_float(x[r].y));
+      } else {
+        st[b0 + rank] = tm;
+        sv[b0 + rank] = __uint_as_float(x[r].y);
+      }
+    }
+  }
+  if (merged) {   // a bath event after the synaptic events at or before it
+    const double *lut = d.lut + (size_t)d.sub[i] * 256;
+    for (uint32_t j = lane; j < bc; j += 32) {
+      const double bt = w.btau[j];
+      const uint32_t b = min((uint32_t)((bt - T0) * (double)HS_BUCKETS), (uint32_t)HS_BUCKETS - 1);
+      uint32_t c = w.start[b];
+      for (uint32_t q = w.start[b]; q < w.start[b + 1]; q++) c += w.tau[q] <= bt;
+      ms[j + c] = make_double2(bt, lut[d.bath_lut[bbase + j]]);
     }
   }
   __syncwarp();   // the warp's next neuron reuses the staging arrays
+  return merged;
 }
 
 #define HEAVY_SORT_THREADS 256
@@ -1861,14 +1904,16 @@ __global__ void __launch_bounds__(HEAVY_SORT_THREADS, 2) heavy_sort_kernel(Dev d
     const uint32_t i = d.heavy_list[hh], n = d.heavy_list[N + hh];
     if (n > wmax) continue;   // not listed here
     uint2 *ev = d.ev + (size_t)i * cap;
+    bool merged;
     if (n <= 32)
-      heavy_sort_one<1>(d, ev, n, t, D, N, cap, lane, ws);
+      merged = heavy_sort_one<1>(d, i, ev, n, t, D, N, cap, lane, ws);
     else if (n <= 64)
-      heavy_sort_one<2>(d, ev, n, t, D, N, cap, lane, ws);
+      merged = heavy_sort_one<2>(d, i, ev, n, t, D, N, cap, lane, ws);
     else if (n <= 128)
-      heavy_sort_one<4>(d, ev, n, t, D, N, cap, lane, ws);
+      merged = heavy_sort_one<4>(d, i, ev, n, t, D, N, cap, lane, ws);
     else
-      heavy_sort_one<8>(d, ev, n, t, D, N, cap, lane, ws);
+      merged = heavy_sort_one<8>(d, i, ev, n, t, D, N, cap, lane, ws);
+    if (merged && lane == 0) d.heavy_list[N + hh] = n | HEAVY_MERGED;
   }
 }
 
@@ -1880,6 +1925,50 @@ __device__ static inline bool huge_runs_here(const NetConst *net, uint32_t cnt) 
   return cnt <= net->ev_cap / 2 && cnt <= MAX_INPUTS_PER_STEP;
 }
 
+// A neuron's merged stream of ne events ({time, input}, in the order they
+// apply): LIFCADynamic over it, four events' loads in flight ahead of the
+// four being applied, each update's coefficients computed off the v/c chain.
+__device__ static inline int run_neuron_merged(const Dev &d, uint32_t i, uint32_t t, const double2 *ms,
+                                               uint32_t ne) {
+  const NetConst *net = d.net;
+  const uint32_t s = d.sub[i];
+  NeuronRegs n;
+  n.v = d.v[i];
+  n.c = d.c[i];
+  n.tr = d.tr[i];
+  n.te = d.te[i];
+  n.fired = 0;
+  const double T0 = (double)t;
+  const double Tau = net->Tau[s], TauC = net->TauC[s];
+  double2 cur[4], nxt[4];
+#pragma unroll
+  for (int u = 0; u < 4; u++) cur[u] = (u < (int)ne) ? ms[u] : make_double2(0.0, 0.0);
+  bool bad = false;
+  for (uint32_t e0 = 0; e0 < ne; e0 += 4) {
+#pragma unroll
+    for (int u = 0; u < 4; u++) nxt[u] = (e0 + 4 + u < ne) ? ms[e0 + 4 + u] : make_double2(0.0, 0.0);
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      if (e0 + u < ne) {
+        const double ct = cur[u].x;
+        double dth, rmh, poly;
+        lifca_coeff(Tau, TauC, ct - n.tr, dth, rmh, poly);
+        bad |= ((ct - T0) >= 1.0) || ((ct - T0) < 0);
+        lifca_pre(net, s, n, ct, cur[u].y, dth, rmh, poly);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) cur[u] = nxt[u];
+  }
+  if (bad) atomicOr(d.flags, F_TIME_WINDOW);
+  d.v[i] = n.v;
+  d.c[i] = n.c;
+  d.tr[i] = n.tr;
+  d.te[i] = n.te;
+  if (n.fired) d.fired[i] = 1;
+  return n.fired;
+}
+
 __global__ void heavy_run_kernel(Dev d) {
   const NetConst *net = d.net;
   const uint32_t t = *d.t, N = net->N, cap = net->ev_cap, wmax = warp_path_max(net);
@@ -1889,6 +1978,12 @@ __global__ void heavy_run_kernel(Dev d) {
     if (hh < nh0) {
       i = d.heavy_list[hh];
       ns = d.heavy_list[N + hh];
+      if (ns & HEAVY_MERGED) {
+        const uint32_t ne = (ns & ~HEAVY_MERGED) + d.bath_cnt[i];
+        if (run_neuron_merged(d, i, t, reinterpret_cast<const double2 *>(d.ev + (size_t)i * cap), ne))
+          atomicAdd(&d.block_fired[i / NEURON_BLOCK], 1u);
+        continue;
+      }
       if (ns > wmax) continue;
     } else {
       i = d.heavy_list[2ull * N + (hh - nh0)];
@@ -2215,8 +2310,28 @@ static int load_logf_fixup(dpsnn_engine *e) {
     uint32_t *dbm;
     DALLOC(dbm, words);
     CK(cudaMemcpyAsync(dbm, bm.data(), 4 * words, cudaMemcpyHostToDevice, e->stream));
-    CK(cudaStreamSynchronize(e->stream));
     e->d.fix_bitmap = dbm;
+    // per result binade, the fix-up inputs' largest distance (ulps) from a
+    // rounding midpoint, with a margin for the device log's last bit
+    std::vector<float> near(256, -1.0f);
+    for (uint32_t key : e->fix_keys) {
+      if (key < 0x30000000u || key > 0x3F800000u) continue;
+      float xf;
+      memcpy(&xf, &key, 4);
+      const double y = log((double)xf);
+      const float f = logf_cr_from(xf, y);
+      uint32_t fb;
+      memcpy(&fb, &f, 4);
+      const uint32_t E = (fb >> 23) & 0xFFu;
+      if ((fb & 0x7FFFFFu) == 0 || E <= 24) continue;   // always checked on the device
+      const double dist = 0.5 - fabs(y - (double)f) * ldexp(1.0, 150 - (int)E);
+      near[E] = std::max(near[E], (float)(dist + 1e-3));
+    }
+    float *dnear;
+    DALLOC(dnear, 256);
+    CK(cudaMemcpyAsync(dnear, near.data(), 4 * 256, cudaMemcpyHostToDevice, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    e->d.fix_near = dnear;
   }
   return 0;
 }
