@@ -585,13 +585,15 @@ __global__ void causal_stdp_kernel(Dev d) {
 // Work item = (delay d, spike q of the slot written d steps ago), i.e. the CSR
 // segment (pre, d).  A warp takes 32 work items at a time: each lane fetches
 // one item's segment bounds, then the warp walks the concatenation of the 32
-// segments with every lane on a different synapse, DELIVER_UNROLL synapses
-// per lane in flight, appending {key, weight} to each target's event list.
+// segments with every lane on a different synapse, appending {key, weight}
+// to each target's event list: per lane a batch of DELIVER_UNROLL synapses
+// takes its slots (atomics) while the next batch's synapse loads are in
+// flight.
 // key = (D-1-d) << 25 | q orders a target's events as the reference delivers
 // them (delay descending, then source ascending), which breaks ties between
 // equal arrival times.
 #define DELIVER_THREADS 256
-#define DELIVER_UNROLL 4
+#define DELIVER_UNROLL 2
 
 // Stores one event in slot s of target j's list (taken by the caller's
 // atomicAdd on ev_cnt[j]), or in the overflow list past the bucket.
@@ -669,33 +671,47 @@ __global__ void __launch_bounds__(DELIVER_THREADS) deliver_kernel(Dev d) {
     ky[lane] = key;
     my_events += len;
     __syncwarp();
-    // the concatenated segments, element e = lane + 32 * i
+    // the concatenated segments, element e = lane + 32 * i, in batches of
+    // DELIVER_UNROLL per lane: the next batch's synapse loads are issued
+    // while this batch's slot atomics are in flight
     uint32_t sg = 0;
+    uint64_t k[DELIVER_UNROLL];
+    uint32_t kk[DELIVER_UNROLL], jj[DELIVER_UNROLL];
+    float wf[DELIVER_UNROLL];
+#define DELIVER_FETCH(E0, K, KK, JJ, WF)                       \
+  _Pragma("unroll") for (int u = 0; u < DELIVER_UNROLL; u++) { \
+    const uint32_t e = (E0) + 32u * u + lane;                 \
+    KK[u] = 0xFFFFFFFFu;                                      \
+    if (e < tot) {                                            \
+      while (off[sg + 1] <= e) sg++;                          \
+      K[u] = bg[sg] + (e - off[sg]);                          \
+      KK[u] = ky[sg];                                         \
+      JJ[u] = __ldg(&d.post[K[u]]);                           \
+      WF[u] = ((float)__ldg(&d.w16[K[u]])) * w2f;             \
+    }                                                         \
+  }
+    DELIVER_FETCH(0u, k, kk, jj, wf);
     for (uint32_t e0 = 0; e0 < tot; e0 += 32u * DELIVER_UNROLL) {
-      uint64_t k[DELIVER_UNROLL];
-      uint32_t kk[DELIVER_UNROLL], jj[DELIVER_UNROLL];
-      float wf[DELIVER_UNROLL];
-#pragma unroll
-      for (int u = 0; u < DELIVER_UNROLL; u++) {
-        const uint32_t e = e0 + 32u * u + lane;
-        kk[u] = 0xFFFFFFFFu;
-        if (e < tot) {
-          while (off[sg + 1] <= e) sg++;
-          k[u] = bg[sg] + (e - off[sg]);
-          kk[u] = ky[sg];
-          jj[u] = __ldg(&d.post[k[u]]);
-          wf[u] = ((float)__ldg(&d.w16[k[u]])) * w2f;
-        }
-      }
-      // all slot atomics in flight before the dependent stores
       uint32_t sl[DELIVER_UNROLL];
 #pragma unroll
       for (int u = 0; u < DELIVER_UNROLL; u++)
         if (kk[u] != 0xFFFFFFFFu) sl[u] = atomicAdd(&d.ev_cnt[jj[u]], 1u);
+      uint64_t nk[DELIVER_UNROLL];
+      uint32_t nkk[DELIVER_UNROLL], njj[DELIVER_UNROLL];
+      float nwf[DELIVER_UNROLL];
+      DELIVER_FETCH(e0 + 32u * DELIVER_UNROLL, nk, nkk, njj, nwf);
 #pragma unroll
       for (int u = 0; u < DELIVER_UNROLL; u++)
         if (kk[u] != 0xFFFFFFFFu) deliver_event(d, net, k[u], kk[u], t, stdp, cap, jj[u], wf[u], sl[u]);
+#pragma unroll
+      for (int u = 0; u < DELIVER_UNROLL; u++) {
+        k[u] = nk[u];
+        kk[u] = nkk[u];
+        jj[u] = njj[u];
+        wf[u] = nwf[u];
+      }
     }
+#undef DELIVER_FETCH
     __syncwarp();
   }
   for (int o = 16; o > 0; o >>= 1) my_events += __shfl_down_sync(0xffffffffu, my_events, o);
@@ -1767,9 +1783,8 @@ __device__ static inline uint32_t warp_path_max(const NetConst *net) {
 
 struct HeavySortWarp {
   uint32_t start[HS_BUCKETS + 1];   // counts, then the buckets' first positions
-  double tau[HEAVY_WARP_MAX];       // events staged by bucket for the counts
-  uint32_t key[HEAVY_WARP_MAX];
-  double btau[HS_BATH_MAX];         // the neuron's bath events (time-ordered)
+  double tau[HEAVY_WARP_MAX + HS_BATH_MAX];   // events staged by bucket for the counts
+  uint32_t key[HEAVY_WARP_MAX + HS_BATH_MAX];
 };
 
 // A heavy neuron's merged event stream in its bucket: {time, input} per
@@ -1780,12 +1795,23 @@ struct HeavySortWarp {
 #define HEAVY_MERGED 0x80000000u
 
 // One heavy neuron's n <= 32*E events (element e = lane + 32r in register r):
-// loaded with their arrival times, sorted by (time, key), written back as
-// sorted times into the bucket's first half and weights into its second half.
+// loaded with their arrival times and sorted by (time, key).  When the
+// merged stream fits half the bucket, the neuron's bath events join the sort
+// with keys above every synaptic key (so a synaptic event comes first on
+// equal times, and bath events keep their order) and the bucket receives the
+// merged stream {time, input}; otherwise it receives the sorted times in its
+// first half and the weights in its second half.  Returns whether merged.
+#define HS_BATH_KEY 0xFFFFFF80u   // + j for bath event j; synaptic keys are below 80 << 25
+static_assert(RING_SLOTS <= 127, "synaptic keys (D-1-d) << 25 | q stay below the bath keys");
+
 template <int E>
 __device__ static inline bool heavy_sort_one(const Dev &d, uint32_t i, uint2 *ev, uint32_t n, uint32_t t, uint32_t D,
                                              uint32_t N, uint32_t cap, uint32_t lane, HeavySortWarp &w) {
   const double T0 = (double)t;
+  const uint32_t bcnt = d.bath_cnt[i];
+  const uint64_t bbase = d.bath_rank_base[i / d.net->locN] + d.bath_off[i];
+  const bool merged = n + bcnt <= cap / 2 && bcnt <= HS_BATH_MAX;
+  const uint32_t bc = merged ? bcnt : 0u;
   for (uint32_t b = lane; b <= HS_BUCKETS; b += 32) w.start[b] = 0;
   uint2 x[E];
 #pragma unroll
@@ -1795,7 +1821,7 @@ __device__ static inline bool heavy_sort_one(const Dev &d, uint32_t i, uint2 *ev
   }
   __syncwarp();
   double tau[E];
-  uint32_t bs[E];   // bucket << 16 | place among the bucket's events in arrival order
+  uint32_t bs[E], bb[HS_BATH_MAX / 32];   // bucket << 16 | place among the bucket's elements in arrival order
 #pragma unroll
   for (int r = 0; r < E; r++) {
     const uint32_t e = lane + 32u * r;
@@ -1805,15 +1831,24 @@ __device__ static inline bool heavy_sort_one(const Dev &d, uint32_t i, uint2 *ev
       bs[r] = (b << 16) | atomicAdd(&w.start[b], 1u);
     }
   }
+#pragma unroll
+  for (int r = 0; r < HS_BATH_MAX / 32; r++) {
+    const uint32_t j = lane + 32u * r;
+    if (j < bc) {
+      const double btj = d.bath_time[bbase + j];
+      const uint32_t b = min((uint32_t)((btj - T0) * (double)HS_BUCKETS), (uint32_t)HS_BUCKETS - 1);
+      bb[r] = (b << 16) | atomicAdd(&w.start[b], 1u);
+    }
+  }
   __syncwarp();
   // exclusive prefix of the counts, 8 consecutive buckets per lane
   {
     uint32_t c[HS_BUCKETS / 32], tot = 0;
 #pragma unroll
-    for (int i = 0; i < HS_BUCKETS / 32; i++) {
-      c[i] = w.start[lane * (HS_BUCKETS / 32) + i];
-      const uint32_t v = c[i];
-      c[i] = tot;
+    for (int q = 0; q < HS_BUCKETS / 32; q++) {
+      c[q] = w.start[lane * (HS_BUCKETS / 32) + q];
+      const uint32_t v = c[q];
+      c[q] = tot;
       tot += v;
     }
     uint32_t incl = tot;
@@ -1822,11 +1857,11 @@ __device__ static inline bool heavy_sort_one(const Dev &d, uint32_t i, uint2 *ev
       if (lane >= (uint32_t)o) incl += y;
     }
 #pragma unroll
-    for (int i = 0; i < HS_BUCKETS / 32; i++) w.start[lane * (HS_BUCKETS / 32) + i] = incl - tot + c[i];
+    for (int q = 0; q < HS_BUCKETS / 32; q++) w.start[lane * (HS_BUCKETS / 32) + q] = incl - tot + c[q];
     if (lane == 31) w.start[HS_BUCKETS] = incl;
   }
   __syncwarp();
-  // staged by bucket; bs becomes bucket << 16 | staged position
+  // staged by bucket; bs/bb become bucket << 16 | staged position
 #pragma unroll
   for (int r = 0; r < E; r++) {
     const uint32_t e = lane + 32u * r;
@@ -1837,15 +1872,30 @@ __device__ static inline bool heavy_sort_one(const Dev &d, uint32_t i, uint2 *ev
       bs[r] = (b << 16) | p;
     }
   }
+#pragma unroll
+  for (int r = 0; r < HS_BATH_MAX / 32; r++) {
+    const uint32_t j = lane + 32u * r;
+    if (j < bc) {
+      const uint32_t b = bb[r] >> 16, p = w.start[b] + (bb[r] & 0xFFFFu);
+      w.tau[p] = d.bath_time[bbase + j];
+      w.key[p] = HS_BATH_KEY + j;
+      bb[r] = (b << 16) | p;
+    }
+  }
   __syncwarp();
-  // the merged stream when it fits half the bucket (16 B per event), else
-  // sorted times and weights in the bucket's halves (heavy_run merges)
-  const uint32_t bc = d.bath_cnt[i];
-  const uint64_t bbase = d.bath_rank_base[i / d.net->locN] + d.bath_off[i];
-  const bool merged = n + bc <= cap / 2 && bc <= HS_BATH_MAX;
-  if (merged)
-    for (uint32_t j = lane; j < bc; j += 32) w.btau[j] = d.bath_time[bbase + j];
-  __syncwarp();
+  // each element's place: its bucket's start plus the bucket's elements
+  // before it in (time, key) order
+  auto place = [&](uint32_t v) -> uint32_t {
+    const uint32_t b = v >> 16, p = v & 0xFFFFu;
+    const uint32_t b0 = w.start[b], b1 = w.start[b + 1], k = w.key[p];
+    const double tm = w.tau[p];
+    uint32_t rank = 0;
+    for (uint32_t j = b0; j < b1; j++) {
+      const double tj = w.tau[j];
+      rank += (tj < tm) || (tj == tm && w.key[j] < k);
+    }
+    return b0 + rank;
+  };
   double2 *ms = reinterpret_cast<double2 *>(ev);
   double *st = reinterpret_cast<double *>(ev);
   float *sv = reinterpret_cast<float *>(ev + cap / 2);
@@ -1853,35 +1903,22 @@ __device__ static inline bool heavy_sort_one(const Dev &d, uint32_t i, uint2 *ev
   for (int r = 0; r < E; r++) {
     const uint32_t e = lane + 32u * r;
     if (e < n) {
-      const uint32_t b = bs[r] >> 16, p = bs[r] & 0xFFFFu;
-      const uint32_t b0 = w.start[b], b1 = w.start[b + 1], k = w.key[p];
-      const double tm = w.tau[p];
-      uint32_t rank = 0;
-      for (uint32_t j = b0; j < b1; j++) {
-        const double tj = w.tau[j];
-        rank += (tj < tm) || (tj == tm && w.key[j] < k);
-      }
-      if (merged) {   // after the bath events strictly before it
-        uint32_t lo = 0, hi = bc;
-        while (lo < hi) {
-          const uint32_t mid = (lo + hi) >> 1;
-          if (w.btau[mid] < tm) lo = mid + 1; else hi = mid;
-        }
-        ms[b0 + rank + lo] = make_double2(tm, (double)__uint_as_float(x[r].y));
+      const uint32_t pos = place(bs[r]);
+      const double tm = w.tau[bs[r] & 0xFFFFu];
+      if (merged) {
+        ms[pos] = make_double2(tm, (double)__uint_as_float(x[r].y));
       } else {
-        st[b0 + rank] = tm;
-        sv[b0 + rank] = __uint_as_float(x[r].y);
+        st[pos] = tm;
+        sv[pos] = __uint_as_float(x[r].y);
       }
     }
   }
-  if (merged) {   // a bath event after the synaptic events at or before it
+  if (merged) {
     const double *lut = d.lut + (size_t)d.sub[i] * 256;
-    for (uint32_t j = lane; j < bc; j += 32) {
-      const double bt = w.btau[j];
-      const uint32_t b = min((uint32_t)((bt - T0) * (double)HS_BUCKETS), (uint32_t)HS_BUCKETS - 1);
-      uint32_t c = w.start[b];
-      for (uint32_t q = w.start[b]; q < w.start[b + 1]; q++) c += w.tau[q] <= bt;
-      ms[j + c] = make_double2(bt, lut[d.bath_lut[bbase + j]]);
+#pragma unroll
+    for (int r = 0; r < HS_BATH_MAX / 32; r++) {
+      const uint32_t j = lane + 32u * r;
+      if (j < bc) ms[place(bb[r])] = make_double2(w.tau[bb[r] & 0xFFFFu], lut[d.bath_lut[bbase + j]]);
     }
   }
   __syncwarp();   // the warp's next neuron reuses the staging arrays
