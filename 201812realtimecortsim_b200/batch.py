@@ -38,7 +38,8 @@ def sweep_configs(n: int, total_ms: int, seed: int = 2024, sides=(1, 2, 3, 4)) -
     """The batched sweep: grid side uniform over ``sides``; per network its
     own seed, external Poisson rate (1-5 kHz: NuExt 1-5 Hz over CExt 1000)
     and calcium adaptation increment (0-2x the baseline 1.0); one reference
-    rank per cortical module."""
+    rank per cortical module; the delay-range sub-population, so that no
+    network is refused for a delay level of 80."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(n):
@@ -46,7 +47,7 @@ def sweep_configs(n: int, total_ms: int, seed: int = 2024, sides=(1, 2, 3, 4)) -
         nu, alpha = float(rng.uniform(1.0, 5.0)), float(rng.uniform(0.0, 2.0))
         kw = {"p1": 0.0376} if g == 2 else {}
         out.append(nc.cortical_grid(g, g, total_ms=total_ms, seed=1 + i, nu_ext_hz=nu, alpha_c=alpha,
-                                    glob_h=g * g, **kw))
+                                    glob_h=g * g, delay_range_subpop=True, **kw))
     return out
 
 

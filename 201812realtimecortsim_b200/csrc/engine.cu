@@ -2006,7 +2006,25 @@ __device__ static inline int run_neuron_merged(const Dev &d, uint32_t i, uint32_
   return n.fired;
 }
 
+// The warp path's neurons whose sort left a merged stream, a thread each.
 __global__ void heavy_run_kernel(Dev d) {
+  const NetConst *net = d.net;
+  const uint32_t t = *d.t, N = net->N, cap = net->ev_cap;
+  const uint32_t nh = min(d.heavy_cnt[0], N);
+  for (uint32_t hh = blockIdx.x * blockDim.x + threadIdx.x; hh < nh; hh += gridDim.x * blockDim.x) {
+    const uint32_t i = d.heavy_list[hh], ns = d.heavy_list[N + hh];
+    if (!(ns & HEAVY_MERGED)) continue;
+    const uint32_t ne = (ns & ~HEAVY_MERGED) + d.bath_cnt[i];
+    if (run_neuron_merged(d, i, t, reinterpret_cast<const double2 *>(d.ev + (size_t)i * cap), ne))
+      atomicAdd(&d.block_fired[i / NEURON_BLOCK], 1u);
+  }
+}
+
+// The other neurons left sorted in their bucket (times and weights in its
+// halves, merged with the bath events here): the warp path's neurons whose
+// merged stream would not fit half the bucket, and the block path's with at
+// most half a bucket of events.  A thread each.
+__global__ void heavy_rest_kernel(Dev d) {
   const NetConst *net = d.net;
   const uint32_t t = *d.t, N = net->N, cap = net->ev_cap, wmax = warp_path_max(net);
   const uint32_t nh0 = min(d.heavy_cnt[0], N), nh = nh0 + min(d.heavy_cnt[1], N);
@@ -2015,13 +2033,7 @@ __global__ void heavy_run_kernel(Dev d) {
     if (hh < nh0) {
       i = d.heavy_list[hh];
       ns = d.heavy_list[N + hh];
-      if (ns & HEAVY_MERGED) {
-        const uint32_t ne = (ns & ~HEAVY_MERGED) + d.bath_cnt[i];
-        if (run_neuron_merged(d, i, t, reinterpret_cast<const double2 *>(d.ev + (size_t)i * cap), ne))
-          atomicAdd(&d.block_fired[i / NEURON_BLOCK], 1u);
-        continue;
-      }
-      if (ns > wmax) continue;
+      if ((ns & HEAVY_MERGED) || ns > wmax) continue;
     } else {
       i = d.heavy_list[2ull * N + (hh - nh0)];
       ns = d.heavy_list[3ull * N + (hh - nh0)];
@@ -2424,6 +2436,27 @@ static void h_gaussian_lut(double mu, double sigma, double xmin, double xmax, do
   }
 }
 
+// The kernels' shared-memory attributes, set once per device and process,
+// before the device's first build: setting an attribute waits for the
+// kernel's running instances, which would serialise the builds of engines
+// built concurrently, and builds with other engines' steps.
+static int set_kernel_attributes(int device) {
+  static std::mutex mu;
+  static std::vector<int> done;
+  std::lock_guard<std::mutex> lock(mu);
+  if ((int)done.size() <= device) done.resize(device + 1, 0);
+  if (done[device]) return 0;
+  CK(cudaFuncSetAttribute(gen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEN_SMEM));
+  CK(cudaFuncSetAttribute(bath_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(BathSmem)));
+  // the bath's blocks stay resident for most of a step: with the largest
+  // shared-memory carveout, the SMs that hold two of them still have room for
+  // a block of the main stream's kernels that use shared memory
+  CK(cudaFuncSetAttribute(bath_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                          (int)cudaSharedmemCarveoutMaxShared));
+  done[device] = 1;
+  return 0;
+}
+
 static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_options *o) {
   NetConst &n = e->hnet;
   memset(&n, 0, sizeof n);
@@ -2580,7 +2613,10 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
   double *dcache;
   TALLOC(dhyp, nmod);
   TALLOC(dcache, nmod);
-  CK(cudaFuncSetAttribute(gen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEN_SMEM));
+  {
+    int rc = set_kernel_attributes(e->device);
+    if (rc) return rc;
+  }
   gen_kernel<<<(2 * nmod + GEN_THREADS - 1) / GEN_THREADS, GEN_THREADS, GEN_SMEM, e->stream>>>(
       d.net, dprob, 0, drec, dhyp, dcache, cnt_out,
                                                           nullptr, nullptr, nullptr, nullptr, scratch,
@@ -2817,12 +2853,6 @@ static int engine_build(dpsnn_engine *e, const dpsnn_params *p, const dpsnn_opti
   e->grid_heavy = (uint32_t)sms * 8;
   e->grid_heavy_run = (uint32_t)sms * 16;
   e->grid_huge = (uint32_t)sms;
-  CK(cudaFuncSetAttribute(bath_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(BathSmem)));
-  // the bath's blocks stay resident for most of a step: with the largest
-  // shared-memory carveout, the SMs that hold two of them still have room for
-  // a block of the main stream's kernels that use shared memory
-  CK(cudaFuncSetAttribute(bath_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
-                          (int)cudaSharedmemCarveoutMaxShared));
   free_temps(e);   // after their last use on this stream
   CK(cudaStreamSynchronize(e->stream));
   return 0;
@@ -3029,6 +3059,9 @@ static int enqueue_step(dpsnn_engine *e) {
   timed_launch_begin(e, 6);
   heavy_run_kernel<<<e->grid_heavy_run, 128, 0, e->stream>>>(d);
   timed_launch_end(e, 6);
+  timed_launch_begin(e, 7);
+  heavy_rest_kernel<<<e->grid_huge, 128, 0, e->stream>>>(d);
+  timed_launch_end(e, 7);
   cudaEventRecord(e->ev_neuron[b], e->stream);
   if (e->hnet.stdp_on) {
     if (d.probe_w && t % 1000 == 999 && t >= e->hnet.start_pl && t <= e->hnet.stop_pl) e->probe_t = t;
@@ -3037,7 +3070,7 @@ static int enqueue_step(dpsnn_engine *e) {
     timed_launch_end(e, 4);
   }
   end_step_kernel<<<1, 1, 0, e->stream>>>(d);
-  e->launches += 9 + (e->hnet.stdp_on ? 2 : 0);
+  e->launches += 10 + (e->hnet.stdp_on ? 2 : 0);
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) return dpsnn_fail(DPSNN_E_CUDA, "kernel launch: %s", cudaGetErrorString(err));
   e->t_host++;

@@ -276,9 +276,11 @@ def poisson_jobs(n_jobs: int, rate_per_s: float, seed: int = 7, max_side: int = 
     external rate, plasticity on for ``stdp_fraction`` of the jobs.  Each job
     is the run of one reference rank per cortical module (env_globH = the
     module count, at most the reference's 256 ranks), so that no emulated
-    rank's serial bath stream is longer than one module.  Grids of 6x6
-    modules and more carry the delay-range sub-population (without it the
-    reference refuses networks of that size)."""
+    rank's serial bath stream is longer than one module.  Every job carries
+    the delay-range sub-population: without it the reference refuses every
+    grid of 6x6 modules and more, and a smaller one now and then (a delay
+    level of 80 has a probability of 6e-8 per synapse); the engine refuses
+    the same networks."""
     rng = np.random.default_rng(seed)
     t = 0.0
     jobs = []
@@ -288,7 +290,7 @@ def poisson_jobs(n_jobs: int, rate_per_s: float, seed: int = 7, max_side: int = 
         dur = int(rng.integers(duration_ms[0], duration_ms[1] + 1))
         stdp = bool(rng.random() < stdp_fraction)
         cfg = nc.cortical_grid(side, side, total_ms=dur, seed=1 + i, nu_ext_hz=float(rng.uniform(*nu_ext_hz)),
-                               stdp=stdp, start_plasticity_ms=0, delay_range_subpop=side >= 6,
+                               stdp=stdp, start_plasticity_ms=0, delay_range_subpop=True,
                                glob_h=side * side, **({"p1": 0.0376} if side == 2 else {}))
         jobs.append(Job(job_id=i, cfg=cfg, duration_ms=dur, arrival_s=t))
     return jobs
