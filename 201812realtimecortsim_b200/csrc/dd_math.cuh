@@ -182,8 +182,8 @@ DD_HD double log_cr(double x) {
 
 // Fix-up table of the C library's logf on (0,1]: sorted input bit patterns
 // keys[] with the library's results vals[]; bucket[b] is the first entry
-// whose key>>12 is >= b + LOGF_FIX_BASE (kept in the file; the engine finds a
-// key through a one-bit-per-float filter and a binary search of keys[]).
+// whose key>>12 is >= b + LOGF_FIX_BASE, so the keys of one block of 4096
+// floats are keys[bucket[b] .. bucket[b+1]).
 #define LOGF_FIX_BASE (0x30000000u >> 12)
 #define LOGF_FIX_NBUCKET ((0x3F800000u >> 12) - LOGF_FIX_BASE + 2)
 typedef struct {

@@ -808,6 +808,7 @@ struct BathSmem {
   unsigned long long chunk_start[BATH_TABS];  // exact start of chunk c (walk, as it begins chunk c)
   uint32_t chunk_seq;               // chunks whose start is published
   uint32_t flag[BATH_ROUNDS];       // round r converted <=> flag[r % BATH_ROUNDS] == r + 1
+  float near[256];                  // the logf fix-up filter's distances (Dev::fix_near)
   uint32_t hist[64];
   unsigned long long pos;           // walk position (draws)
   unsigned long long raw_end;       // draws generated
@@ -824,12 +825,24 @@ __device__ __forceinline__ uint32_t bath_row(uint32_t dl) {
   return min(__funnelshift_r(dl, dl, 1), (uint32_t)BATH_NC);
 }
 
+// The fix-up value of input key (when it has one), else f: a binary search of
+// the keys of its block of 4096 floats.
+__device__ static inline float logf_fixup_search(const logf_fixup_t &fx, uint32_t key, float f) {
+  const uint32_t bk = (key >> 12) - LOGF_FIX_BASE;
+  uint32_t lo = __ldg(&fx.bucket[bk]), hi = __ldg(&fx.bucket[bk + 1]);
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(&fx.keys[mid]) < key) lo = mid + 1; else hi = mid;
+  }
+  return (lo < fx.n && __ldg(&fx.keys[lo]) == key) ? __ldg(&fx.vals[lo]) : f;
+}
+
 // logf of the host C library on (0,1].  The inputs where it differs from
 // the correctly rounded float all have an exact logarithm close to a
 // rounding midpoint; an input whose logarithm lies farther from one than any
 // fix-up input of the same result binade returns the correctly rounded value
 // at once.  Otherwise a one-bit-per-float filter, then a binary search of
-// the fix-up keys.
+// the fix-up keys of its block of 4096 floats.
 __device__ static inline float logf_ref_dev(const logf_fixup_t &fx, const uint32_t *__restrict__ bitmap,
                                             const float *__restrict__ near, float x) {
   const double y = log((double)x);
@@ -846,12 +859,7 @@ __device__ static inline float logf_ref_dev(const logf_fixup_t &fx, const uint32
   }
   const uint32_t bit = key - 0x30000000u;
   if (!((__ldg(&bitmap[bit >> 5]) >> (bit & 31)) & 1u)) return f;
-  uint32_t lo = 0, hi = fx.n;
-  while (lo < hi) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (__ldg(&fx.keys[mid]) < key) lo = mid + 1; else hi = mid;
-  }
-  return (lo < fx.n && __ldg(&fx.keys[lo]) == key) ? __ldg(&fx.vals[lo]) : f;
+  return logf_fixup_search(fx, key, f);
 }
 
 // Converts raw draw mj into (LUT index, lapse) (getPoissonLapse, :844-865,
@@ -862,6 +870,40 @@ __device__ static inline float bath_lapse(const Dev &d, uint32_t mj, uint8_t &id
   double temp = (double)1.0 - u;
   if (temp < 0) temp = 0;
   return -logf_ref_dev(d.fix, d.fix_bitmap, d.fix_near, (float)temp);
+}
+
+// bath_lapse for three draws at once, each step for all three before the
+// next: their filter-table loads are in flight together.  near is the
+// per-binade distance table (logf_ref_dev), here from shared memory.
+__device__ static inline void bath_lapse3(const Dev &d, const float *near, const uint32_t (&mj)[3], float (&lap)[3],
+                                          uint8_t (&idx)[3]) {
+  float f[3];
+  uint32_t key[3], bw[3];
+  bool chk[3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    const double u = mj[i] * (1.0 / (double)MBIG);
+    idx[i] = (uint8_t)(uint32_t)(u * 256);
+    double temp = (double)1.0 - u;
+    if (temp < 0) temp = 0;
+    const float x = (float)temp;
+    const double y = log((double)x);
+    f[i] = logf_cr_from(x, y);
+    key[i] = __float_as_uint(x);
+    chk[i] = key[i] >= 0x30000000u && key[i] <= 0x3F800000u;
+    const uint32_t fb = __float_as_uint(f[i]), E = (fb >> 23) & 0xFFu;
+    if (chk[i] && (fb & 0x7FFFFFu) != 0 && E > 24) {
+      const double inv_ulp = __longlong_as_double((long long)(150 - E + 1023) << 52);   // 2^(150-E)
+      chk[i] = 0.5 - fabs(y - (double)f[i]) * inv_ulp <= (double)near[E];
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 3; i++) bw[i] = chk[i] ? __ldg(&d.fix_bitmap[(key[i] - 0x30000000u) >> 5]) : 0u;
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    if ((bw[i] >> ((key[i] - 0x30000000u) & 31)) & 1u) f[i] = logf_fixup_search(d.fix, key[i], f[i]);
+    lap[i] = -f[i];
+  }
 }
 
 __device__ static inline uint32_t lap_fixed(float lap) {
@@ -963,6 +1005,7 @@ __global__ void __launch_bounds__(BATH_THREADS, 2) bath_kernel(Dev d) {
     s.idx[k] = d.draw_idx[(size_t)h * BATH_RING + k];
   }
   for (uint32_t r = tid; r < BATH_ROUNDS; r += blockDim.x) s.flag[r] = 0;
+  for (uint32_t r = tid; r < 256; r += blockDim.x) s.near[r] = d.fix_near[r];
   if (tid == 0) {
     s.pos = p0;
     s.raw_end = q0;
@@ -1121,49 +1164,51 @@ __global__ void __launch_bounds__(BATH_THREADS, 2) bath_kernel(Dev d) {
       // in turn (quad 8c + k to builder (8c + k) mod BATH_BUILDERS), so each
       // builder takes four quads in three chunks and needs no other warp
       for (uint32_t k = (bw + BATH_BUILDERS - (8 * c) % BATH_BUILDERS) % BATH_BUILDERS; k < 8; k += BATH_BUILDERS) {
-        // stage 1: the quad's neurons j = 4k .. 4k+3; for neuron j the lanes
-        // take the candidates o = lane and lane + 32.  For a start P the
-        // count is m + 1, m the number of i < 32 whose sum of the i+1
-        // lapses at P+1, P+3, .., P+1+2i is below lo (the sums grow with
-        // i), when the (m+1)-th sum reaches hi1.  Positions are taken
-        // modulo 2^32 (a step reads far fewer draws); the two candidates'
-        // binary searches run in lockstep.
-        for (uint32_t j = 4 * k; j < 4 * k + 4; j++) {
+        // stage 1: the quad's neurons j = 4k .. 4k+3, two at a time (a half
+        // warp each); for neuron j the half's lanes take the candidates
+        // o = hl, hl + 16, hl + 32, hl + 48.  For a start P the count is
+        // m + 1, m the number of i < 32 whose sum of the i+1 lapses at P+1,
+        // P+3, .., P+1+2i is below lo (the sums grow with i), when the
+        // (m+1)-th sum reaches hi1.  Positions are taken modulo 2^32 (a step
+        // reads far fewer draws); the four candidates' binary searches run
+        // in lockstep.
+        for (uint32_t jp = 4 * k; jp < 4 * k + 4; jp += 2) {
+          const uint32_t hl = lane & 15u, j = jp + (lane >> 4);
           const uint32_t mj = __shfl_sync(0xffffffffu, misc, j);
           const uint32_t loj = __shfl_sync(0xffffffffu, lo, j), hij = __shfl_sync(0xffffffffu, hi1, j);
           const uint32_t bj = __shfl_sync(0xffffffffu, b32, j);
           uint8_t *row = s.tab[b][j];
           if (!mj) {   // no bath event this step (or past the rank's last neuron): 0 from any start
-            row[lane] = 0;
-            row[lane + 32] = 0;
-            continue;
-          }
-          const uint32_t cap = mj & 0xFFu;
-          // draw P+1+2i of a candidate sits at word hv | ((w0 + i) mod 4096) of q[]
-          const uint32_t hv = ((bj + 1) & 1u) * (BATH_RING / 2);
-          uint32_t w0[2], qb[2], m[2];
-          bool ok[2];
 #pragma unroll
-          for (int v = 0; v < 2; v++) {
-            const uint32_t P = bj + 2u * (lane + 32u * v);
-            ok[v] = (int32_t)(P - f32) >= 0 && (int32_t)(r32 - P) >= 0;
-            w0[v] = (P + 1) >> 1;
-            qb[v] = s.q[hv | ((w0[v] - 1) & (BATH_RING / 2 - 1))];
-            m[v] = 0;
-          }
+            for (int v = 0; v < 4; v++) row[hl + 16 * v] = 0;
+          } else {
+            const uint32_t cap = mj & 0xFFu;
+            // draw P+1+2i of a candidate sits at word hv | ((w0 + i) mod 4096) of q[]
+            const uint32_t hv = ((bj + 1) & 1u) * (BATH_RING / 2);
+            uint32_t w0[4], qb[4], m[4];
+            bool ok[4];
 #pragma unroll
-          for (uint32_t st = 16; st > 0; st >>= 1) {
-            uint32_t f[2];
+            for (int v = 0; v < 4; v++) {
+              const uint32_t P = bj + 2u * (hl + 16u * v);
+              ok[v] = (int32_t)(P - f32) >= 0 && (int32_t)(r32 - P) >= 0;
+              w0[v] = (P + 1) >> 1;
+              qb[v] = s.q[hv | ((w0[v] - 1) & (BATH_RING / 2 - 1))];
+              m[v] = 0;
+            }
 #pragma unroll
-            for (int v = 0; v < 2; v++) f[v] = s.q[hv | ((w0[v] + m[v] + st - 1) & (BATH_RING / 2 - 1))];
+            for (uint32_t st = 16; st > 0; st >>= 1) {
+              uint32_t f[4];
 #pragma unroll
-            for (int v = 0; v < 2; v++) m[v] += (f[v] - qb[v] < loj) ? st : 0u;
-          }
+              for (int v = 0; v < 4; v++) f[v] = s.q[hv | ((w0[v] + m[v] + st - 1) & (BATH_RING / 2 - 1))];
 #pragma unroll
-          for (int v = 0; v < 2; v++) {
-            const uint32_t F = s.q[hv | ((w0[v] + m[v]) & (BATH_RING / 2 - 1))] - qb[v];
-            const uint32_t mm = (m[v] == 31 && F < loj) ? 32u : m[v];
-            row[lane + 32 * v] = (ok[v] && mm < cap && F >= hij) ? (uint8_t)(mm + 1) : (uint8_t)0xFF;
+              for (int v = 0; v < 4; v++) m[v] += (f[v] - qb[v] < loj) ? st : 0u;
+            }
+#pragma unroll
+            for (int v = 0; v < 4; v++) {
+              const uint32_t F = s.q[hv | ((w0[v] + m[v]) & (BATH_RING / 2 - 1))] - qb[v];
+              const uint32_t mm = (m[v] == 31 && F < loj) ? 32u : m[v];
+              row[hl + 16 * v] = (ok[v] && mm < cap && F >= hij) ? (uint8_t)(mm + 1) : (uint8_t)0xFF;
+            }
           }
         }
         // the quad's window bases, and each table's answer outside its
@@ -1238,11 +1283,14 @@ __global__ void __launch_bounds__(BATH_THREADS, 2) bath_kernel(Dev d) {
       uint8_t ix[3];
       float lp[3];
       uint32_t v[3];
+      {
+        uint32_t raw[3];
 #pragma unroll
-      for (int i = 0; i < 3; i++) {
-        lp[i] = bath_lapse(d, vs.lap[(n0 + lane + 32 * i) & M], ix[i]);
-        v[i] = lap_fixed(lp[i]);
+        for (int i = 0; i < 3; i++) raw[i] = vs.lap[(n0 + lane + 32 * i) & M];
+        bath_lapse3(d, s.near, raw, lp, ix);
       }
+#pragma unroll
+      for (int i = 0; i < 3; i++) v[i] = lap_fixed(lp[i]);
       // per-parity prefix over the 96 draws: within each 32, then the
       // totals of the earlier 32s (lanes 30, 31) carried
       for (int o = 2; o < 32; o <<= 1) {
