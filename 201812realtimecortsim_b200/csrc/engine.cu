@@ -729,7 +729,7 @@ __global__ void __launch_bounds__(DELIVER_THREADS) deliver_kernel(Dev d) {
 //              and the lapse factor -logf((float)(1-u)), and extend q[], the
 //              running sum over draws of one parity of the lapses in 2^-20
 //              units (q[n] = q[n-2] + round(lap[n] * 2^20), integers mod 2^32);
-//   warps 5-7, 9-11 (builders) tabulate the event counts of the chunk of 32
+//   warps 5-7, 9-15 (builders) tabulate the event counts of the chunk of 32
 //              neurons two chunks ahead of the walk.  The number of events c
 //              of a neuron is the first c at which nextBath + sum of c lapses
 //              * invNuExt reaches t+1; it depends on where in the stream the
@@ -760,7 +760,7 @@ __global__ void __launch_bounds__(DELIVER_THREADS) deliver_kernel(Dev d) {
 //              the walk shares its scheduler with the emitter only.
 // Rounds are published in order with a flag; every wait is bounded and
 // raises F_BATH_DRAWS when its limit is reached.
-#define BATH_THREADS 384       // 12 warps: roles in bath_kernel
+#define BATH_THREADS 512       // 16 warps: roles in bath_kernel
 #define BATH_RING 8192         // draws resident in shared memory
 #define BATH_ROUNDS 512        // round flags tracked (BATH_ROUNDS*24 > BATH_RING)
 #define BATH_MAX_EXT 2048      // largest maxExternCurrentCount supported
@@ -768,7 +768,7 @@ __global__ void __launch_bounds__(DELIVER_THREADS) deliver_kernel(Dev d) {
 #define BATH_FAST_LANES 32     // events decided by one count table entry
 #define BATH_WINDOW (2 * BATH_FAST_LANES + 2)   // draws a count decision reads past its start
 #define BATH_NC 64             // candidate start positions tabulated per neuron
-#define BATH_BUILDERS 6        // table-building warps: 5, 6, 7, 9, 10, 11
+#define BATH_BUILDERS 10       // table-building warps: 5, 6, 7, 9 .. 15
 #define BATH_AHEAD 2           // chunks the count tables are built ahead of the consumer (the code below
                                // predicts from chunk c-2's start)
 #define BATH_TABS (BATH_AHEAD + 1)
@@ -985,7 +985,7 @@ __device__ static inline unsigned long long bath_exact(BathSmem &s, double nbv, 
 }
 
 __device__ static inline int bath_builder_index(uint32_t warp) {
-  return (warp >= 5 && warp <= 7) ? (int)warp - 5 : (warp >= 9 && warp <= 11) ? (int)warp - 6 : -1;
+  return (warp >= 5 && warp <= 7) ? (int)warp - 5 : (warp >= 9 && warp <= 15) ? (int)warp - 6 : -1;
 }
 
 __global__ void __launch_bounds__(BATH_THREADS, 2) bath_kernel(Dev d) {
@@ -1161,8 +1161,8 @@ __global__ void __launch_bounds__(BATH_THREADS, 2) bath_kernel(Dev d) {
       const uint32_t b32 = (uint32_t)base, f32 = (uint32_t)floor_pos;
       const uint32_t r32 = (uint32_t)reach - BATH_WINDOW;
       // this warp's quads of the chunk: the rank's quads go to the builders
-      // in turn (quad 8c + k to builder (8c + k) mod BATH_BUILDERS), so each
-      // builder takes four quads in three chunks and needs no other warp
+      // in turn (quad 8c + k to builder (8c + k) mod BATH_BUILDERS), so the
+      // builders share the quads evenly and need no other warp
       for (uint32_t k = (bw + BATH_BUILDERS - (8 * c) % BATH_BUILDERS) % BATH_BUILDERS; k < 8; k += BATH_BUILDERS) {
         // stage 1: the quad's neurons j = 4k .. 4k+3, two at a time (a half
         // warp each); for neuron j the half's lanes take the candidates
@@ -2918,9 +2918,13 @@ extern "C" int dpsnn_create(const dpsnn_params *p, const dpsnn_options *opts, dp
   } else {
     cudaGetDevice(&e->device);
   }
+  // The bath of the next step runs beside this step's kernels and has a
+  // step of slack; the main stream's blocks go first when both wait for room.
+  int prio_least = 0, prio_greatest = 0;
   bool ok = cudaSetDevice(e->device) == cudaSuccess &&
-            cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) == cudaSuccess &&
-            cudaStreamCreateWithFlags(&e->bath_stream, cudaStreamNonBlocking) == cudaSuccess;
+            cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest) == cudaSuccess &&
+            cudaStreamCreateWithPriority(&e->stream, cudaStreamNonBlocking, prio_greatest) == cudaSuccess &&
+            cudaStreamCreateWithPriority(&e->bath_stream, cudaStreamNonBlocking, prio_least) == cudaSuccess;
   for (int b = 0; b < 2 && ok; b++)
     ok = cudaEventCreateWithFlags(&e->ev_bath[b], cudaEventDisableTiming) == cudaSuccess &&
          cudaEventCreateWithFlags(&e->ev_neuron[b], cudaEventDisableTiming) == cudaSuccess;
