@@ -573,7 +573,11 @@ __global__ void causal_stdp_kernel(Dev d) {
       int32_t la = d.last_act[s];
       int td = (int)t - 1 - la;
       float fc = (la != 0 && td < 128) ? net->causal_tab[td] : 0.0f;
-      d.tderiv[s] = d.tderiv[s] + fc;
+      // the reference adds the term even when it is zero
+      // (DPSNN_neuron_sim.c:171); a time derivative is never -0.0 (it starts
+      // at +0.0 and no step of the plasticity makes a -0.0 from other
+      // values), so skipping the zero terms changes no bit
+      if (fc != 0.0f) d.tderiv[s] = d.tderiv[s] + fc;
       if (d.stdp_log && fc != 0.0f && t != 0 && i < net->locN && s < d.row_ptr[net->locN])
         stdp_log_append(d, s, i, 0u, fc);
     }
@@ -613,7 +617,7 @@ __device__ static inline void deliver_event(const Dev &d, const NetConst *net, u
     d.last_act[k] = (int32_t)t;
     const int td = (int)t - d.last_spike_ms[j];
     const float a = (td < 128) ? net->anti_tab[td] : 0.0f;
-    d.tderiv[k] = d.tderiv[k] + a;
+    if (a != 0.0f) d.tderiv[k] = d.tderiv[k] + a;   // zero terms change no bit (causal_stdp_kernel)
   }
 }
 
@@ -1719,7 +1723,7 @@ __device__ static inline int run_neuron_se(const Dev &d, uint32_t i, uint32_t t,
 // Heavier neurons are queued for the heavy path below.
 __device__ static inline uint32_t warp_path_max(const NetConst *net);
 
-__global__ void __launch_bounds__(NEURON_BLOCK) neuron_kernel(Dev d) {
+__global__ void __launch_bounds__(NEURON_BLOCK, 4) neuron_kernel(Dev d) {
   const NetConst *net = d.net;
   const uint32_t t = *d.t, N = net->N, D = net->D, cap = net->ev_cap;
   const uint32_t i = blockIdx.x * NEURON_BLOCK + threadIdx.x;
