@@ -1980,8 +1980,14 @@ __device__ static inline bool heavy_sort_one(const Dev &d, uint32_t i, uint2 *ev
 #define HEAVY_SORT_THREADS 256
 
 // A warp per neuron of the warp path (LOCAL_EVENTS < n <= HEAVY_WARP_MAX),
-// each warp with its own bucket-sort arrays in shared memory.
-__global__ void __launch_bounds__(HEAVY_SORT_THREADS, 2) heavy_sort_kernel(Dev d) {
+// each warp with its own bucket-sort arrays in shared memory.  Two kernels
+// over the same list: up to 64 events (one or two per lane, the common case
+// outside bursts) at four blocks per SM, more events (four or eight per lane,
+// more registers) at two.
+#define HEAVY_SORT_SMALL 64
+
+template <bool SMALL>
+__device__ static inline void heavy_sort_list(const Dev &d) {
   __shared__ HeavySortWarp s_ws[HEAVY_SORT_THREADS / 32];
   const NetConst *net = d.net;
   const uint32_t t = *d.t, N = net->N, D = net->D, cap = net->ev_cap, wmax = warp_path_max(net);
@@ -1991,20 +1997,27 @@ __global__ void __launch_bounds__(HEAVY_SORT_THREADS, 2) heavy_sort_kernel(Dev d
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t hh = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; hh < nh; hh += nwarps) {
     const uint32_t i = d.heavy_list[hh], n = d.heavy_list[N + hh];
-    if (n > wmax) continue;   // not listed here
+    // not listed here (sorted already, by the other kernel, flags the count)
+    if (n > wmax || (SMALL ? n > HEAVY_SORT_SMALL : n <= HEAVY_SORT_SMALL)) continue;
     uint2 *ev = d.ev + (size_t)i * cap;
     bool merged;
-    if (n <= 32)
-      merged = heavy_sort_one<1>(d, i, ev, n, t, D, N, cap, lane, ws);
-    else if (n <= 64)
-      merged = heavy_sort_one<2>(d, i, ev, n, t, D, N, cap, lane, ws);
-    else if (n <= 128)
-      merged = heavy_sort_one<4>(d, i, ev, n, t, D, N, cap, lane, ws);
-    else
-      merged = heavy_sort_one<8>(d, i, ev, n, t, D, N, cap, lane, ws);
+    if (SMALL) {
+      if (n <= 32)
+        merged = heavy_sort_one<1>(d, i, ev, n, t, D, N, cap, lane, ws);
+      else
+        merged = heavy_sort_one<2>(d, i, ev, n, t, D, N, cap, lane, ws);
+    } else {
+      if (n <= 128)
+        merged = heavy_sort_one<4>(d, i, ev, n, t, D, N, cap, lane, ws);
+      else
+        merged = heavy_sort_one<8>(d, i, ev, n, t, D, N, cap, lane, ws);
+    }
     if (merged && lane == 0) d.heavy_list[N + hh] = n | HEAVY_MERGED;
   }
 }
+
+__global__ void __launch_bounds__(HEAVY_SORT_THREADS, 4) heavy_sort_kernel(Dev d) { heavy_sort_list<true>(d); }
+__global__ void __launch_bounds__(HEAVY_SORT_THREADS, 2) heavy_sort_big_kernel(Dev d) { heavy_sort_list<false>(d); }
 
 // Runs a neuron whose events were left sorted in its bucket (arrival times,
 // then weights): the warp path's neurons, and the block path's neurons with
@@ -3108,6 +3121,7 @@ static int enqueue_step(dpsnn_engine *e) {
   timed_launch_end(e, 3);
   timed_launch_begin(e, 5);
   heavy_sort_kernel<<<e->grid_heavy, HEAVY_SORT_THREADS, 0, e->stream>>>(d);
+  heavy_sort_big_kernel<<<e->grid_heavy, HEAVY_SORT_THREADS, 0, e->stream>>>(d);
   timed_launch_end(e, 5);
   timed_launch_begin(e, 7);
   huge_kernel<<<e->grid_huge, HEAVY_THREADS, 0, e->stream>>>(d);
@@ -3126,7 +3140,7 @@ static int enqueue_step(dpsnn_engine *e) {
     timed_launch_end(e, 4);
   }
   end_step_kernel<<<1, 1, 0, e->stream>>>(d);
-  e->launches += 10 + (e->hnet.stdp_on ? 2 : 0);
+  e->launches += 11 + (e->hnet.stdp_on ? 2 : 0);
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) return dpsnn_fail(DPSNN_E_CUDA, "kernel launch: %s", cudaGetErrorString(err));
   e->t_host++;
