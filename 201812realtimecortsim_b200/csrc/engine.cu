@@ -2072,7 +2072,7 @@ __device__ static inline int run_neuron_merged(const Dev &d, uint32_t i, uint32_
 }
 
 // The warp path's neurons whose sort left a merged stream, a thread each.
-__global__ void heavy_run_kernel(Dev d) {
+__global__ void __launch_bounds__(128, 6) heavy_run_kernel(Dev d) {
   const NetConst *net = d.net;
   const uint32_t t = *d.t, N = net->N, cap = net->ev_cap;
   const uint32_t nh = min(d.heavy_cnt[0], N);
