@@ -651,8 +651,13 @@ __global__ void __launch_bounds__(DELIVER_THREADS) deliver_kernel(Dev d) {
     uint64_t beg = 0;
     uint32_t len = 0, key = 0;
     if (w < total) {
-      uint32_t dl = 0;
-      while (s_pre[dl + 1] <= w) dl++;
+      // the delay level: the first dl with s_pre[dl + 1] > w (binary search
+      // over the D levels, some of them empty)
+      uint32_t dl = 0, hi = D - 1;
+      while (dl < hi) {
+        const uint32_t mid = (dl + hi) >> 1;
+        if (s_pre[mid + 1] <= w) dl = mid + 1; else hi = mid;
+      }
       const uint32_t q = w - s_pre[dl];
       const uint32_t slot = (t + RING_SLOTS - dl) % RING_SLOTS;
       const uint32_t P = d.ring_ids[(size_t)slot * N + q];
@@ -1995,24 +2000,51 @@ __device__ static inline void heavy_sort_list(const Dev &d) {
   HeavySortWarp &ws = s_ws[threadIdx.x >> 5];
   const uint32_t nh = min(d.heavy_cnt[0], N);
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t hh = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; hh < nh; hh += nwarps) {
-    const uint32_t i = d.heavy_list[hh], n = d.heavy_list[N + hh];
-    // not listed here (sorted already, by the other kernel, flags the count)
-    if (n > wmax || (SMALL ? n > HEAVY_SORT_SMALL : n <= HEAVY_SORT_SMALL)) continue;
-    uint2 *ev = d.ev + (size_t)i * cap;
-    bool merged;
-    if (SMALL) {
-      if (n <= 32)
-        merged = heavy_sort_one<1>(d, i, ev, n, t, D, N, cap, lane, ws);
-      else
-        merged = heavy_sort_one<2>(d, i, ev, n, t, D, N, cap, lane, ws);
-    } else {
-      if (n <= 128)
-        merged = heavy_sort_one<4>(d, i, ev, n, t, D, N, cap, lane, ws);
-      else
-        merged = heavy_sort_one<8>(d, i, ev, n, t, D, N, cap, lane, ws);
+  // a neuron not listed here was sorted already by the other kernel, which
+  // flags the count
+  auto mine = [&](uint32_t n) { return n <= wmax && (SMALL ? n <= HEAVY_SORT_SMALL : n > HEAVY_SORT_SMALL); };
+  // the warp's list entries are read two neurons ahead, and the next
+  // neuron's events are prefetched into L2 while this one is sorted
+  uint32_t hh = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  uint32_t i = 0, n = 0, i1 = 0, n1 = 0;
+  if (hh < nh) {
+    i = d.heavy_list[hh];
+    n = d.heavy_list[N + hh];
+  }
+  if (hh + nwarps < nh) {
+    i1 = d.heavy_list[hh + nwarps];
+    n1 = d.heavy_list[N + hh + nwarps];
+  }
+  for (; hh < nh; hh += nwarps) {
+    const uint32_t h2 = hh + 2u * nwarps;
+    uint32_t i2 = 0, n2 = 0;
+    if (h2 < nh) {
+      i2 = d.heavy_list[h2];
+      n2 = d.heavy_list[N + h2];
     }
-    if (merged && lane == 0) d.heavy_list[N + hh] = n | HEAVY_MERGED;
+    // 16 events (128 bytes) per lane's line, inside neuron i1's bucket
+    if (hh + nwarps < nh && mine(n1) && lane * 16u < n1)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(d.ev + (size_t)i1 * cap + lane * 16u));
+    if (mine(n)) {
+      uint2 *ev = d.ev + (size_t)i * cap;
+      bool merged;
+      if (SMALL) {
+        if (n <= 32)
+          merged = heavy_sort_one<1>(d, i, ev, n, t, D, N, cap, lane, ws);
+        else
+          merged = heavy_sort_one<2>(d, i, ev, n, t, D, N, cap, lane, ws);
+      } else {
+        if (n <= 128)
+          merged = heavy_sort_one<4>(d, i, ev, n, t, D, N, cap, lane, ws);
+        else
+          merged = heavy_sort_one<8>(d, i, ev, n, t, D, N, cap, lane, ws);
+      }
+      if (merged && lane == 0) d.heavy_list[N + hh] = n | HEAVY_MERGED;
+    }
+    i = i1;
+    n = n1;
+    i1 = i2;
+    n1 = n2;
   }
 }
 
