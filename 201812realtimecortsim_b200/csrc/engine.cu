@@ -650,14 +650,17 @@ __global__ void __launch_bounds__(DELIVER_THREADS) deliver_kernel(Dev d) {
     const uint32_t w = w0 + lane;
     uint64_t beg = 0;
     uint32_t len = 0, key = 0;
+    // the delay level of item w: the first dl with s_pre[dl + 1] > w.  The
+    // warp finds w0's by a binary search over the D levels (some of them
+    // empty), the same for every lane; each lane steps on from there (its 32
+    // items span few levels)
+    uint32_t dl = 0, hi = D - 1;
+    while (dl < hi) {
+      const uint32_t mid = (dl + hi) >> 1;
+      if (s_pre[mid + 1] <= w0) dl = mid + 1; else hi = mid;
+    }
     if (w < total) {
-      // the delay level: the first dl with s_pre[dl + 1] > w (binary search
-      // over the D levels, some of them empty)
-      uint32_t dl = 0, hi = D - 1;
-      while (dl < hi) {
-        const uint32_t mid = (dl + hi) >> 1;
-        if (s_pre[mid + 1] <= w) dl = mid + 1; else hi = mid;
-      }
+      while (s_pre[dl + 1] <= w) dl++;
       const uint32_t q = w - s_pre[dl];
       const uint32_t slot = (t + RING_SLOTS - dl) % RING_SLOTS;
       const uint32_t P = d.ring_ids[(size_t)slot * N + q];
