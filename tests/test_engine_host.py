@@ -126,3 +126,54 @@ def _has_gpu():
 def test_create_fails_loudly_without_gpu():
     with pytest.raises(E.EngineError, match="CUDA"):
         E.Engine(CASES["small_1x1"]())
+
+
+def test_entry_points_reject_null_arguments():
+    """Every entry point that takes an engine, a graph or an output pointer
+    checks it before it touches the device: DPSNN_E_PARAM (-1) with a message,
+    0 from the accessors, nothing from the destructors."""
+    lib = E.load_library()
+    E_PARAM = -1
+    u32 = C.c_uint32(0)
+    P = C.c_void_p
+    calls = {
+        "dpsnn_create": lambda: lib.dpsnn_create(None, None, None),
+        "dpsnn_step": lambda: lib.dpsnn_step(None, 1),
+        "dpsnn_sync": lambda: lib.dpsnn_sync(None),
+        "dpsnn_step_many": lambda: lib.dpsnn_step_many(None, 2, 1),
+        "dpsnn_spikes": lambda: lib.dpsnn_spikes(None, 0, None, None, 0, C.byref(u32)),
+        "dpsnn_spikes_range": lambda: lib.dpsnn_spikes_range(None, 0, 1, None, None, 0, None),
+        "dpsnn_rank_spikes_noalloc": lambda: lib.dpsnn_rank_spikes_noalloc(None, 0, 0, None, None, 0, C.byref(u32)),
+        "dpsnn_state": lambda: lib.dpsnn_state(None, None, None, None, None, None),
+        "dpsnn_bath_params": lambda: lib.dpsnn_bath_params(None, None, None),
+        "dpsnn_backward_synapses": lambda: lib.dpsnn_backward_synapses(None, 0, None, None, None, None, None, None),
+        "dpsnn_enable_ltp_probe": lambda: lib.dpsnn_enable_ltp_probe(None),
+        "dpsnn_ltp_probe": lambda: lib.dpsnn_ltp_probe(None, 0, None, None, None, None, None),
+        "dpsnn_enable_stdp_events": lambda: lib.dpsnn_enable_stdp_events(None),
+        "dpsnn_stdp_events": lambda: lib.dpsnn_stdp_events(None, None, None, None, None, 0, C.byref(u32)),
+        "dpsnn_set_timing": lambda: lib.dpsnn_set_timing(None, 1),
+        "dpsnn_kernel_times": lambda: lib.dpsnn_kernel_times(None, None, None),
+        "dpsnn_graph_run": lambda: lib.dpsnn_graph_run(None),
+        "dpsnn_set_launch_shape": lambda: lib.dpsnn_set_launch_shape(None, 0, 0, 0),
+    }
+    for name, call in calls.items():
+        assert call() == E_PARAM, name
+        assert lib.dpsnn_last_error(), name
+    for name in ("dpsnn_glob_n", "dpsnn_time_ms", "dpsnn_synapse_count", "dpsnn_events_delivered",
+                 "dpsnn_device_bytes", "dpsnn_kernel_launches"):
+        assert getattr(lib, name)(None) == 0, name
+    assert lib.dpsnn_rank_synapse_count(None, 0) == 0
+    assert lib.dpsnn_cuda_stream(None) is None
+    lib.dpsnn_destroy(None)
+    lib.dpsnn_graph_destroy(None)
+    # a graph holds a positive multiple of the 80 ring slots of at least one
+    # engine; these are refused before any engine is read
+    g = P()
+    assert lib.dpsnn_graph_create(None, 0, 80, C.byref(g)) == E_PARAM and not g.value
+    eng = (P * 1)(None)
+    assert lib.dpsnn_graph_create(eng, 1, 40, C.byref(g)) == E_PARAM and not g.value
+    assert b"multiple of 80" in lib.dpsnn_last_error()
+    assert lib.dpsnn_graph_create(eng, 1, 80, C.byref(g)) == E_PARAM
+    assert b"null engine 0" in lib.dpsnn_last_error()
+    assert lib.dpsnn_step_many(eng, 1, 1) == E_PARAM
+    assert b"null engine 0" in lib.dpsnn_last_error()
